@@ -1,0 +1,59 @@
+// Fused time-step kernels (stencil_fused.cu): two kernels per time step for a
+// batch of shots sharing one model.
+//   fused_p_step: pressure stencil + Hicks injection (gather form) + stage-B
+//                 extended source + p = px + pz + free surface, and the
+//                 deferred store of the previous step's velocity history;
+//   fused_v_step: velocity stencil + stage-B extended sources + free surface,
+//                 the deferred store of this step's pressure history, and the
+//                 receiver / datum Hicks gathers in extra CTAs.
+// Histories are FP32 or FP16 with one power-of-two scale per shot, step and
+// field, chosen from that step's max |value| (reduced by the kernel that
+// produces the field and applied by the kernel that reads it next).
+#pragma once
+
+#include "kernels.cuh"
+
+namespace daw {
+
+enum FusedMode { FM_FWD = 0, FM_STAGE_A = 1, FM_STAGE_B = 2, FM_STAGE_B_ES = 3 };
+
+constexpr int kAmaxSlots = 32;  // spread of the max-|x| atomics
+
+struct ShotDevice {
+  float *px, *pz, *vx, *vz, *p;  // extended-grid state [n2e][ld]
+  void* hist;                    // [nt][3][n2][n1h] (float or __half)
+  unsigned* amax;                // [nt][3][kAmaxSlots] max-|x| bit patterns
+  const float* amp;              // wavelet (forward) or res(nt,nr) (stage A)
+  int amp_stride;                // 0 for the wavelet, nt for res
+  InjMapDev inj;                 // source (forward) or receiver (stage A) map
+  StationsDev rec;               // receivers for the gathers
+  float* out;                    // sis(nt,nr) (forward / stage B)
+  int out_reverse;               // 1: row nt-it (MINRES operator output)
+  StationsDev datum;             // datum receivers (may be empty)
+  float* red;                    // datum gather (nt, ndatum), accumulated (+=)
+  float* wf;                     // optional (n1,n2,nt) pressure history
+  int wf_acc;                    // 1: wf += p (final esource), 0: wf = p
+  int nt;                        // this shot's record length
+  int type_src, type_rec;
+  int active;                    // 0 = skip this shot
+  double* cost;                  // optional sum of 0.5*sp^2 (final esource)
+};
+
+struct FusedLaunch {
+  const ShotDevice* shots;  // device array
+  int nshots;
+  int hist_fp16;
+  int n1h;                  // history leading dimension
+  int chunk;                // columns per warp
+  int max_rec, max_datum;   // largest station counts (gather CTAs)
+};
+
+// Stage-A flush at it = nt+1 is folded into fused_p_step (it may exceed a
+// shot's nt by one in stage A).
+void fused_p_step(const Grid& g, const ModelDev& m, const FusedLaunch& L, int mode, int it,
+                  cudaStream_t st);
+void fused_v_step(const Grid& g, const ModelDev& m, const FusedLaunch& L, int mode, int it,
+                  cudaStream_t st);
+int fused_warps(const Grid& g, int chunk);
+
+}  // namespace daw
