@@ -183,6 +183,9 @@ int daw_run_parfile(daw_handle* h, const char* workdir, int32_t first, int32_t l
 /* Timing of the last pipeline call: device milliseconds by phase. */
 typedef struct daw_timing {
   double forward_ms, operator_ms, minres_vec_ms, esource_ms, filter_ms, total_ms;
+  double sim_fwd_ms, sim_a_ms, sim_b_ms;  /* device time of the time loops by kind */
+  double steps_fwd, steps_a, steps_b;     /* time steps launched (batch-wide) */
+  double shot_steps;          /* shot time steps (sum over shots of batch steps) */
   double point_updates;       /* extended-grid point updates performed */
   double hist_bytes;          /* history bytes written + read */
   int64_t kernel_launches;    /* kernels launched by the library */

@@ -71,7 +71,9 @@ class Timing(C.Structure):
     _fields_ = [("forward_ms", C.c_double), ("operator_ms", C.c_double),
                 ("minres_vec_ms", C.c_double), ("esource_ms", C.c_double),
                 ("filter_ms", C.c_double), ("total_ms", C.c_double),
-                ("point_updates", C.c_double), ("hist_bytes", C.c_double),
+                ("sim_fwd_ms", C.c_double), ("sim_a_ms", C.c_double), ("sim_b_ms", C.c_double),
+                ("steps_fwd", C.c_double), ("steps_a", C.c_double), ("steps_b", C.c_double),
+                ("shot_steps", C.c_double), ("point_updates", C.c_double), ("hist_bytes", C.c_double),
                 ("kernel_launches", C.c_int64)]
 
 

@@ -400,13 +400,20 @@ float* hist32(daw_handle* h, ShotCtx& c, int it1, int field) {
   return static_cast<float*>(c.hist) + ((size_t)(it1 - 1) * 3 + field) * ni;
 }
 
-void store_hist_plain(daw_handle* h, float* dst, const float* src) {
-  // interior -> [n2][n1h]: reuse the compact store with n1 = n1h layout via a
-  // temporary grid whose n1 is the history leading dimension is not possible,
-  // so store compact n1 x n2 into the padded slice row by row through k_store
-  // semantics: the plain port keeps n1h == n1 layout by storing with ld n1.
-  plain_store_interior(h->g, dst, src, false, h->st);
-}
+// Device time of one time loop (events on the library stream).
+struct SimClock {
+  daw_handle* h;
+  explicit SimClock(daw_handle* hh) : h(hh) { CK(cudaEventRecord(h->ev0, h->st)); }
+  void stop(double* ms, double* steps, double nsteps, double shot_steps) {
+    CK(cudaEventRecord(h->ev1, h->st));
+    CK(cudaEventSynchronize(h->ev1));
+    float t = 0;
+    CK(cudaEventElapsedTime(&t, h->ev0, h->ev1));
+    *ms += t;
+    *steps += nsteps;
+    h->tim.shot_steps += shot_steps;
+  }
+};
 
 void plain_forward(daw_handle* h, ShotCtx& c, float* sis, float* wf, float* red) {
   const Grid& g = h->g;
@@ -415,6 +422,7 @@ void plain_forward(daw_handle* h, ShotCtx& c, float* sis, float* wf, float* red)
   CK(cudaMemsetAsync(sis, 0, (size_t)c.nt * c.nr * sizeof(float), h->st));
   if (red) CK(cudaMemsetAsync(red, 0, (size_t)c.nt * h->ndatum * sizeof(float), h->st));
   const size_t ni = g.int_elems();
+  SimClock clk(h);
   for (int it = 1; it <= c.nt; ++it) {
     plain_p_update(g, h->md, f, 2, +1, h->st);
     if (c.type_src == 0) plain_inject(c.srcmap, c.px, h->md.kap, g.dt, c.d_s + (it - 1), 0, +1, h->st);
@@ -432,6 +440,7 @@ void plain_forward(daw_handle* h, ShotCtx& c, float* sis, float* wf, float* red)
     h->tim.kernel_launches += 6;
   }
   check_launch("plain forward");
+  clk.stop(&h->tim.sim_fwd_ms, &h->tim.steps_fwd, c.nt, c.nt);
   h->tim.point_updates += (double)c.nt * g.n1e * g.n2e;
 }
 
@@ -439,6 +448,7 @@ void plain_stage_a(daw_handle* h, ShotCtx& c, const float* res) {
   const Grid& g = h->g;
   PlainFields f{c.p, c.px, c.pz, c.vx, c.vz};
   zero_state(h, c);
+  SimClock clk(h);
   for (int it = 1; it <= c.nt; ++it) {
     plain_p_update(g, h->md, f, 3, -1, h->st);
     plain_inject(c.recmap, c.px, h->md.kap, g.dt, res + (it - 1), c.nt, -1, h->st);
@@ -451,6 +461,7 @@ void plain_stage_a(daw_handle* h, ShotCtx& c, const float* res) {
     h->tim.kernel_launches += 8;
   }
   check_launch("plain stage A");
+  clk.stop(&h->tim.sim_a_ms, &h->tim.steps_a, c.nt, c.nt);
   h->tim.point_updates += (double)c.nt * g.n1e * g.n2e;
   h->tim.hist_bytes += (double)c.nt * 3 * g.int_elems() * 4;
 }
@@ -463,6 +474,7 @@ void plain_stage_b(daw_handle* h, ShotCtx& c, bool esource, float* out, int reve
   CK(cudaMemsetAsync(out, 0, (size_t)c.nt * c.nr * sizeof(float), h->st));
   if (red) CK(cudaMemsetAsync(red, 0, (size_t)c.nt * h->ndatum * sizeof(float), h->st));
   const size_t ni = g.int_elems();
+  SimClock clk(h);
   for (int it = 1; it <= c.nt; ++it) {
     const int ic = c.nt - it + 1;
     plain_p_update(g, h->md, f, 3, +1, h->st);
@@ -482,6 +494,7 @@ void plain_stage_b(daw_handle* h, ShotCtx& c, bool esource, float* out, int reve
     h->tim.kernel_launches += 7;
   }
   check_launch("plain stage B");
+  clk.stop(&h->tim.sim_b_ms, &h->tim.steps_b, c.nt, c.nt);
   h->tim.point_updates += (double)c.nt * g.n1e * g.n2e;
   h->tim.hist_bytes += (double)c.nt * 3 * g.int_elems() * 4;
 }
@@ -559,6 +572,15 @@ FusedLaunch launch_of(daw_handle* h, Batch& b) {
 // Runs `nsteps` steps of `mode`, captured once per batch/mode in a CUDA
 // graph when enabled (kernel arguments are constant; per-shot pointers live in
 // the device-side ShotDevice array, refreshed before each replay).
+void stop_clock(daw_handle* h, SimClock& clk, Batch& b, int mode) {
+  double shot_steps = 0;
+  for (ShotCtx* c : b.shots)
+    if (c->active) shot_steps += c->nt;
+  double* ms = mode == FM_FWD ? &h->tim.sim_fwd_ms : mode == FM_STAGE_A ? &h->tim.sim_a_ms : &h->tim.sim_b_ms;
+  double* st = mode == FM_FWD ? &h->tim.steps_fwd : mode == FM_STAGE_A ? &h->tim.steps_a : &h->tim.steps_b;
+  clk.stop(ms, st, b.max_nt, shot_steps);
+}
+
 void run_fused(daw_handle* h, Batch& b, int mode) {
   const Grid& g = h->g;
   FusedLaunch L = launch_of(h, b);
@@ -586,9 +608,13 @@ void run_fused(daw_handle* h, Batch& b, int mode) {
       cudaGraphDestroy(graph);
       it = h->graphs.emplace(key, exec).first;
     }
+    SimClock clk(h);
     CK(cudaGraphLaunch(it->second, h->st));
+    stop_clock(h, clk, b, mode);
   } else {
+    SimClock clk(h);
     body();
+    stop_clock(h, clk, b, mode);
   }
   check_launch("fused steps");
   h->tim.kernel_launches += launches;
@@ -1177,6 +1203,12 @@ int daw_create(daw_handle** out, int32_t device) {
     return DAW_ERR_CUDA;
   }
   apply_preset(h->opt, 1);
+  if (cudaEventCreate(&h->ev0) != cudaSuccess || cudaEventCreate(&h->ev1) != cudaSuccess) {
+    cudaGetLastError();
+    cudaStreamDestroy(h->st);
+    delete h;
+    return DAW_ERR_CUDA;
+  }
   *out = h;
   return DAW_OK;
 }
@@ -1188,6 +1220,8 @@ void daw_destroy(daw_handle* h) {
   drop_graphs(h);
   h->pool.clear();
   h->model_pool.clear();
+  if (h->ev0) cudaEventDestroy(h->ev0);
+  if (h->ev1) cudaEventDestroy(h->ev1);
   cudaStreamDestroy(h->st);
   delete h;
 }

@@ -65,12 +65,16 @@ def test_ggt_bitexact(pkg, O, case, preset, opt):
 def test_esource_bitexact(pkg, O, case, preset, opt):
     w = case["w"]
     res = np.asfortranarray(case["dobs"][::-1])
-    ref, refwf, refcost = O.esource(w.c0, w.npml, w.h, w.ofs, w.nt, w.dt, res, case["rec"])
+    ref, refwf, _ = O.esource(w.c0, w.npml, w.h, w.ofs, w.nt, w.dt, res, case["rec"])
     with handle(pkg, case, preset, **opt) as h:
         sis, wf, cost = h.submodeling_adjoint_esource(res, case["rec"])
     assert np.array_equal(sis, ref)
     assert np.array_equal(wf, refwf)
-    assert abs(cost - refcost) <= 1e-5 * abs(refcost)
+    # `cost` is accumulated in FP64 on the device; the reference's sequential
+    # FP32 sum of ~2e6 terms is itself off by ~1e-3, so compare with FP64
+    _, _, cost64 = O.esource(w.c0, w.npml, w.h, w.ofs, w.nt, w.dt, res.astype(np.float64),
+                             case["rec"], prec="f64", want_wavefield=False)
+    assert abs(cost - cost64) <= 1e-5 * abs(cost64)
 
 
 def test_ggt_fp16_history(pkg, O, case):
