@@ -89,14 +89,18 @@ def test_ggt_fp16_history(pkg, O, case):
 
 
 def test_ggt_power_of_two_linearity(pkg, case):
-    """Size-independent identity: A(2x) == 2 A(x) bit for bit, also with FP16
-    histories (their per-step scales are powers of two)."""
+    """Size-independent identity: A(2x) == 2 A(x), also with FP16 histories
+    (their per-step scales are powers of two).  Exact except for values in
+    the FP32 subnormal range (the stencil's exponentially small precursors
+    ahead of the wavefront), where doubling is not exact."""
     res = np.asfortranarray(case["dobs"][::-1])
     for preset, opt in (("plain", {}), ("mixed", {})):
         with handle(pkg, case, preset, **opt) as h:
             g1 = h.submodeling_adjoint_esource_data(res, case["rec"])
             g2 = h.submodeling_adjoint_esource_data(2 * res, case["rec"])
-        assert np.array_equal(g2, 2 * g1), preset
+        assert rel_l2(g2, 2 * g1) <= 1e-12, preset
+        big = np.abs(g1) > 1e-30 * np.abs(g1).max()
+        assert np.array_equal(g2[big], 2 * g1[big]), preset
 
 
 @pytest.mark.parametrize("preset,opt,prec,tol", [
@@ -124,30 +128,35 @@ def _shot(case, w):
 
 
 @pytest.fixture(scope="module")
-def oracle_shot(O, case):
+def oracle_shots(O, case):
     w = case["w"]
-    return O.daw_shot(w.c0, w.npml, w.h, w.ofs, w.nt, w.dt, case["s"], case["src"],
-                      case["rec"], case["dobs"], w.mu, w.maxiter, 0.0, case["ird"], w.band,
-                      prec="f64")
+    return {p: O.daw_shot(w.c0, w.npml, w.h, w.ofs, w.nt, w.dt, case["s"], case["src"],
+                          case["rec"], case["dobs"], w.mu, w.maxiter, 0.0, case["ird"], w.band,
+                          prec=p) for p in ("f32", "f64")}
 
 
-@pytest.mark.parametrize("preset,opt,tol", [("plain", {}, FP32_TOL), ("mixed", {}, MIXED_TOL),
-                                            ("mixed", {"history": 0}, FP32_TOL)])
-def test_shot_pipeline(pkg, case, oracle_shot, preset, opt, tol):
+# The FP32 paths are held to the FP32 oracle (the reference computes in REAL):
+# forward data and residuals bit for bit, MINRES and after within 1e-4 (its
+# inner products are parallel reductions).  The FP16-history path is held to
+# the FP64 oracle within 1e-3.  (FP32 against FP64 is limited by cancellation
+# in dobs - datar, a property of the reference's own precision.)
+@pytest.mark.parametrize("preset,opt,prec,tol", [("plain", {}, "f32", FP32_TOL),
+                                                 ("mixed", {}, "f64", MIXED_TOL),
+                                                 ("mixed", {"history": 0}, "f32", FP32_TOL)])
+def test_shot_pipeline(pkg, case, oracle_shots, preset, opt, prec, tol):
     w = case["w"]
     with handle(pkg, case, preset, **opt) as h:
         h.set_datum(case["ird"])
         out = h.shot(**_shot(case, w))
-    ref = oracle_shot
-    assert rel_l2(out["datar"], ref["datar"]) <= 1e-6
-    assert rel_l2(out["deltadr"], ref["deltadr"]) <= 1e-6
-    for k in ("deltade", "dataesc", "datae", "redatumed_raw"):
+    ref = oracle_shots[prec]
+    if prec == "f32":
+        assert np.array_equal(out["datar"], ref["datar"])
+        assert np.array_equal(out["deltadr"], ref["deltadr"])
+    else:
+        assert rel_l2(out["datar"], ref["datar"]) <= 1e-6
+    for k in ("deltade", "dataesc", "datae", "redatumed_raw", "redatumed"):
         err = rel_l2(out[k], ref[k])
         assert err <= tol, (k, err)
-    # the filter's own error budget is ~1e-7 (single-precision temporaries of
-    # the reference's FFT); the redatumed output inherits the simulation's
-    err = rel_l2(out["redatumed"], ref["redatumed"])
-    assert err <= tol, err
     assert out["minres"]["itn"] == w.maxiter
 
 
@@ -210,7 +219,9 @@ def test_edge_stations_and_options(pkg, O, preset):
     rng = np.random.default_rng(9)
     vp = np.asfortranarray((1700 + rng.uniform(-40, 40, (n1, n2))).astype(np.float32))
     s = (np.sin(np.arange(nt) * 0.3) * np.exp(-0.03 * np.arange(nt))).astype(np.float32)
-    pos = [[0.0, 0.0], [5.0, 490.0], [350.0, 0.0], [350.0, 490.0], [-60.0, 250.0],
+    # z = -4 m lies above the free surface (all ten upper taps mirrored);
+    # x = -50 m and x = 540 m put stations in the side sponges
+    pos = [[0.0, 0.0], [5.0, 490.0], [350.0, 0.0], [350.0, 490.0], [-4.0, 250.0],
            [170.0, -50.0], [100.0, 540.0], [400.0, 250.0]]
     for ofs in (0, 1):
         rec = O.acqui_table(pos, h, npml, ofs)
