@@ -512,7 +512,7 @@ struct Batch {
 
 int chunk_of(const daw_handle* h) {
   if (h->opt.chunk > 0) return h->opt.chunk;
-  return 16;
+  return 2;
 }
 
 void fill_shot_devices(daw_handle* h, Batch& b, int mode) {
@@ -1247,7 +1247,8 @@ int daw_set_option(daw_handle* h, int32_t key, double value) {
       case DAW_OPT_SKIP_DEAD_OP: h->opt.skip_dead_op = v ? 1 : 0; break;
       case DAW_OPT_MAX_BATCH: h->opt.max_batch = std::max(0, v); break;
       case DAW_OPT_CHUNK:
-        if (v < 0 || v > 256) throw DawError{DAW_ERR_ARG, "chunk out of range"};
+        if (v != 0 && v != 1 && v != 2 && v != 4)
+          throw DawError{DAW_ERR_ARG, "points per thread must be 1, 2 or 4 (0 = default)"};
         h->opt.chunk = v;
         break;
       default: throw DawError{DAW_ERR_ARG, "unknown option"};

@@ -25,6 +25,48 @@ __device__ __forceinline__ float dplus(float fm1, float f0, float fp1, float fp2
   return fadd(fmul(kA0, fsub(fp1, f0)), fmul(kA1, fsub(fp2, fm1)));
 }
 
+// Hicks gather of station s by one warp, summed in the reference's order
+// (i1 outer, i2 inner; src/submodeling2.f90:214-219).  The lanes form the 441
+// products c*f in parallel into `prod` (shared, 444 floats, 16-byte aligned);
+// lane 0 then adds them in order.  Taps outside the support clipped to
+// [1,hi1]x[1,hi2] contribute +0, which leaves every partial sum's value
+// unchanged.  Returns the sum on lane 0.
+__device__ __forceinline__ float warp_gather_ordered(float* prod, const int* ix1p,
+                                                     const int* ix2p, const float* tiles, int s,
+                                                     const float* __restrict__ origin, int ld,
+                                                     int shift, int hi1, int hi2) {
+  const int lane = threadIdx.x & 31;
+  const int ix1 = __ldg(ix1p + s) - shift, ix2 = __ldg(ix2p + s) - shift;
+  const int r1a = max(1 - ix1, -kRad), r1b = min(hi1 - ix1, kRad);
+  const int r2a = max(1 - ix2, -kRad), r2b = min(hi2 - ix2, kRad);
+  const float* tile = tiles + (size_t)s * kTile;
+  for (int t = lane; t < 444; t += 32) {
+    float v = 0.f;
+    if (t < kTile) {
+      const int a = t / kTap - kRad, b = t % kTap - kRad;
+      if (a >= r1a && a <= r1b && b >= r2a && b <= r2b)
+        v = fmul(__ldg(tile + (a + kRad) + kTap * (b + kRad)),
+                 origin[(ix1 + a - 1) + (size_t)ld * (ix2 + b - 1)]);
+    }
+    prod[t] = v;
+  }
+  __syncwarp();
+  float acc = 0.f;
+  if (lane == 0) {
+    const float4* p4 = reinterpret_cast<const float4*>(prod);
+#pragma unroll 4
+    for (int q = 0; q < 111; ++q) {
+      const float4 v = p4[q];
+      acc = fadd(acc, v.x);
+      acc = fadd(acc, v.y);
+      acc = fadd(acc, v.z);
+      acc = fadd(acc, v.w);
+    }
+  }
+  __syncwarp();
+  return acc;
+}
+
 // ---------------------------------------------------------------------------
 // Launch wrappers (stencil_plain.cu): the literal port, one kernel per
 // reference loop nest.  Indices are 0-based; reference index I = i + 1.

@@ -125,33 +125,15 @@ constexpr int kGatherWarps = 8;
 __global__ void __launch_bounds__(kGatherWarps * 32)
     k_gather(StationsDev st, const float* __restrict__ origin, int ld, int shift, int hi1,
              int hi2, float* __restrict__ out, int out_stride, int row, size_t field_stride) {
-  __shared__ float prod[kGatherWarps][kTile];
+  __shared__ __align__(16) float prod[kGatherWarps][444];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   const int s = blockIdx.x * kGatherWarps + wib;
   const int t_row = blockIdx.y;  // history index when batching rows
   if (s >= st.n) return;
   const float* f = origin + field_stride * t_row;
-  const int ix1 = st.ix1[s] - shift, ix2 = st.ix2[s] - shift;
-  const int r1a = max(1 - ix1, -kRad), r1b = min(hi1 - ix1, kRad);
-  const int r2a = max(1 - ix2, -kRad), r2b = min(hi2 - ix2, kRad);
-  const float* tile = st.tile + (size_t)s * kTile;
-  for (int t = lane; t < kTile; t += 32) {
-    const int i1 = t / kTap - kRad, i2 = t % kTap - kRad;
-    float v = 0.0f;
-    if (i1 >= r1a && i1 <= r1b && i2 >= r2a && i2 <= r2b) {
-      // tile is stored [i1+10 + 21*(i2+10)]
-      const float c = tile[(i1 + kRad) + kTap * (i2 + kRad)];
-      v = fmul(c, f[(ix1 + i1 - 1) + (size_t)ld * (ix2 + i2 - 1)]);
-    }
-    prod[wib][t] = v;
-  }
-  __syncwarp();
-  if (lane == 0) {
-    float acc = 0.0f;
-    for (int i1 = r1a; i1 <= r1b; ++i1)
-      for (int i2 = r2a; i2 <= r2b; ++i2) acc = fadd(acc, prod[wib][(i1 + kRad) * kTap + (i2 + kRad)]);
-    out[(row + t_row) + (size_t)out_stride * s] = acc;
-  }
+  const float acc = warp_gather_ordered(prod[wib], st.ix1, st.ix2, st.tile, s, f, ld, shift,
+                                        hi1, hi2);
+  if (lane == 0) out[(row + t_row) + (size_t)out_stride * s] = acc;
 }
 
 dim3 grid2(int n1, int n2) { return dim3((n1 + kBX - 1) / kBX, (n2 + kBY - 1) / kBY); }

@@ -37,7 +37,7 @@ def handle(pkg, case, preset="plain", **opt):
 
 
 PATHS = [("plain", {}), ("mixed", {"history": 0}), ("mixed", {"history": 0, "graph": 0}),
-         ("mixed", {"history": 0, "chunk": 5})]
+         ("mixed", {"history": 0, "chunk": 1}), ("mixed", {"history": 0, "chunk": 4})]
 
 
 @pytest.mark.parametrize("preset,opt", PATHS)
