@@ -52,7 +52,7 @@ std::string shot_name(int i);  // subname: 5-digit zero padded
 // ---------------------------------------------------------------------------
 struct Grid {
   int n1, n2, npml, n1e, n2e;
-  int ld;        // leading dimension of extended-grid fields (floats), %32 == 0
+  int ld;        // leading dimension of extended-grid fields (floats), %64 == 0
   int ofs;
   float h, dt, dtdx;
   __host__ __device__ size_t ext_elems() const { return (size_t)ld * n2e; }

@@ -22,7 +22,8 @@ namespace daw {
 void minres_log_f32(MinresDev<float>* d, double* log, const float* x, cudaStream_t st);
 void minres_log_f64(MinresDev<double>* d, double* log, const float* x, cudaStream_t st);
 void history_cost(const void* hist, int fp16, const unsigned* amax, int nt, int n1, int n2,
-                  int inner_ld, size_t field_stride, double* out, cudaStream_t st);
+                  int inner_ld, int inner_off, size_t field_stride, double* out,
+                  cudaStream_t st);
 }  // namespace daw
 
 namespace {
@@ -367,7 +368,9 @@ InjMapDev make_map(daw_handle* h, Pool& pool, const std::string& name, const int
 // ---------------------------------------------------------------------------
 int hist_ld(const daw_handle* h) {
   // interior rows per column, padded to 8 elements (16 B of FP16)
-  return (h->g.n1 + 7) / 8 * 8;
+  // interior rows + 1 (the fused layout shifts rows by npml & 1 so a lane's
+  // row pair is aligned), padded to 8 elements (16 B of FP16)
+  return (h->g.n1 + 1 + 7) / 8 * 8;
 }
 size_t hist_bytes_per_step(const daw_handle* h, bool fp16) {
   return (size_t)3 * hist_ld(h) * h->g.n2 * (fp16 ? 2 : 4);
@@ -658,7 +661,7 @@ void batch_operator(daw_handle* h, Batch& b, bool esource) {
       if (!c->active) continue;
       plain_stage_a(h, *c, c->op_in);
       if (esource && c->d_cost) {
-        history_cost(c->hist, 0, nullptr, c->nt, h->g.n1, h->g.n2, h->g.n1,
+        history_cost(c->hist, 0, nullptr, c->nt, h->g.n1, h->g.n2, h->g.n1, 0,
                      (size_t)hist_ld(h) * h->g.n2, c->d_cost, h->st);
       }
       plain_stage_b(h, *c, esource, c->op_out, c->op_reverse, esource ? c->d_wf : nullptr,
@@ -677,7 +680,7 @@ void batch_operator(daw_handle* h, Batch& b, bool esource) {
     if (!c->active) continue;
     if (esource && c->d_cost)
       history_cost(c->hist, h->opt.history_fp16, c->amax, c->nt, h->g.n1, h->g.n2, hist_ld(h),
-                   (size_t)hist_ld(h) * h->g.n2, c->d_cost, h->st);
+                   h->g.npml & 1, (size_t)hist_ld(h) * h->g.n2, c->d_cost, h->st);
     zero_state(h, *c);
     CK(cudaMemsetAsync(c->op_out, 0, (size_t)c->nt * c->nr * sizeof(float), h->st));
     if (esource && h->ndatum)
@@ -1289,7 +1292,7 @@ int daw_set_model(daw_handle* h, const float* vp, int32_t n1, int32_t n2, int32_
     Grid g{};
     g.n1 = n1; g.n2 = n2; g.npml = npml;
     g.n1e = n1 + 2 * npml; g.n2e = n2 + 2 * npml;
-    g.ld = (g.n1e + 31) / 32 * 32;
+    g.ld = (g.n1e + 63) / 64 * 64;  // fused kernels: 64 rows (32 lanes x float2) per warp
     g.ofs = ofs;
     g.h = hgrid; g.dt = dt; g.dtdx = dt / hgrid;
     std::vector<float> d1a, d1a1, d1b, d1b1, d2a, d2a1, d2b, d2b1;
