@@ -191,6 +191,9 @@ struct daw_handle {
   std::vector<std::vector<int32_t>> staged_rec;
   std::vector<ShotCtx> staged_ctx;
   int staged_ready = 0;
+  // TMA kernels: persistent grid sizes and the bounded-wait error flag
+  int persist_p = 0, persist_v = 0;
+  unsigned* d_err = nullptr;
 };
 
 namespace {
@@ -508,15 +511,15 @@ void plain_stage_b(daw_handle* h, ShotCtx& c, bool esource, float* out, int reve
 struct Batch {
   std::vector<ShotCtx*> shots;
   ShotDevice* d_shots = nullptr;
+  TmaMaps* d_maps = nullptr;
   std::vector<ShotDevice> h_shots;
   int max_nt = 0, max_rec = 0, max_datum = 0;
   int slot0 = 0;
 };
 
-int chunk_of(const daw_handle* h) {
-  if (h->opt.chunk > 0) return h->opt.chunk;
-  return 2;
-}
+// 0: TMA-pipelined persistent kernels (default); 1, 2, 4: register kernels
+// with that many columns per thread.
+int chunk_of(const daw_handle* h) { return h->opt.chunk; }
 
 void fill_shot_devices(daw_handle* h, Batch& b, int mode) {
   b.h_shots.resize(b.shots.size());
@@ -558,6 +561,19 @@ void fill_shot_devices(daw_handle* h, Batch& b, int mode) {
     }
   }
   upload(b.d_shots, b.h_shots.data(), b.h_shots.size() * sizeof(ShotDevice), h->st);
+  if (chunk_of(h) == 0) {
+    // tensor maps of every shot's fields (the TMA kernels' operands)
+    std::vector<TmaMaps> maps(b.shots.size());
+    for (size_t i = 0; i < b.shots.size(); ++i) {
+      const ShotCtx& c = *b.shots[i];
+      if (!tma_encode_maps(h->g, c.vx, c.vz, c.px, c.pz, c.p, h->md.kap, &maps[i]))
+        throw DawError{DAW_ERR_CUDA, "cuTensorMapEncodeTiled failed"};
+    }
+    b.d_maps = static_cast<TmaMaps*>(
+        h->pool.get("batch.maps" + std::to_string(b.slot0), maps.size() * sizeof(TmaMaps)));
+    upload(b.d_maps, maps.data(), maps.size() * sizeof(TmaMaps), h->st);
+    sync(h);  // `maps` goes out of scope
+  }
 }
 
 FusedLaunch launch_of(daw_handle* h, Batch& b) {
@@ -569,7 +585,20 @@ FusedLaunch launch_of(daw_handle* h, Batch& b) {
   L.chunk = chunk_of(h);
   L.max_rec = b.max_rec;
   L.max_datum = b.max_datum;
+  L.maps = b.d_maps;
+  L.err = h->d_err;
+  L.persist_p = h->persist_p;
+  L.persist_v = h->persist_v;
   return L;
+}
+
+void check_device_error(daw_handle* h) {
+  unsigned e = 0;
+  CK(cudaMemcpy(&e, h->d_err, sizeof e, cudaMemcpyDeviceToHost));
+  if (e) {
+    CK(cudaMemset(h->d_err, 0, sizeof(unsigned)));
+    throw DawError{DAW_ERR_TIMEOUT, "a bounded device wait ran out (TMA tile copy did not complete)"};
+  }
 }
 
 // Runs `nsteps` steps of `mode`, captured once per batch/mode in a CUDA
@@ -588,18 +617,24 @@ void run_fused(daw_handle* h, Batch& b, int mode) {
   const Grid& g = h->g;
   FusedLaunch L = launch_of(h, b);
   const int last = (mode == FM_STAGE_A) ? b.max_nt + 1 : b.max_nt;  // +1: history flush
+  const bool tma = L.chunk == 0;
   auto body = [&]() {
     for (int it = 1; it <= last; ++it) {
-      fused_p_step(g, h->md, L, mode, it, h->st);
-      if (it <= b.max_nt) fused_v_step(g, h->md, L, mode, it, h->st);
+      if (tma) {
+        tma_p_step(g, h->md, L, mode, it, h->st);
+        if (it <= b.max_nt) tma_v_step(g, h->md, L, mode, it, h->st);
+      } else {
+        fused_p_step(g, h->md, L, mode, it, h->st);
+        if (it <= b.max_nt) fused_v_step(g, h->md, L, mode, it, h->st);
+      }
     }
   };
   const long long launches = 2LL * b.max_nt + (mode == FM_STAGE_A ? 1 : 0);
   if (h->opt.graph) {
     char key[256];
-    std::snprintf(key, sizeof key, "m%d.n%d.s%zu.p%p.c%d.f%d.r%d.d%d", mode, b.max_nt,
-                  b.shots.size(), (void*)b.d_shots, L.chunk, L.hist_fp16, L.max_rec,
-                  L.max_datum);
+    std::snprintf(key, sizeof key, "m%d.n%d.s%zu.p%p.q%p.c%d.f%d.r%d.d%d", mode, b.max_nt,
+                  b.shots.size(), (void*)b.d_shots, (void*)b.d_maps, L.chunk, L.hist_fp16,
+                  L.max_rec, L.max_datum);
     auto it = h->graphs.find(key);
     if (it == h->graphs.end()) {
       cudaGraph_t graph;
@@ -620,6 +655,7 @@ void run_fused(daw_handle* h, Batch& b, int mode) {
     stop_clock(h, clk, b, mode);
   }
   check_launch("fused steps");
+  if (tma) check_device_error(h);
   h->tim.kernel_launches += launches;
   for (ShotCtx* c : b.shots)
     if (c->active) h->tim.point_updates += (double)c->nt * g.n1e * g.n2e;
@@ -1212,6 +1248,14 @@ int daw_create(daw_handle** out, int32_t device) {
     delete h;
     return DAW_ERR_CUDA;
   }
+  tma_prepare(&h->persist_p, &h->persist_v);
+  if (cudaMalloc(&h->d_err, sizeof(unsigned)) != cudaSuccess ||
+      cudaMemset(h->d_err, 0, sizeof(unsigned)) != cudaSuccess || cudaGetLastError() != cudaSuccess) {
+    cudaGetLastError();
+    cudaStreamDestroy(h->st);
+    delete h;
+    return DAW_ERR_CUDA;
+  }
   *out = h;
   return DAW_OK;
 }
@@ -1225,6 +1269,7 @@ void daw_destroy(daw_handle* h) {
   h->model_pool.clear();
   if (h->ev0) cudaEventDestroy(h->ev0);
   if (h->ev1) cudaEventDestroy(h->ev1);
+  if (h->d_err) cudaFree(h->d_err);
   cudaStreamDestroy(h->st);
   delete h;
 }

@@ -11,6 +11,11 @@
 // produces the field and applied by the kernel that reads it next).
 #pragma once
 
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
+#include <algorithm>
+
 #include "kernels.cuh"
 
 namespace daw {
@@ -39,14 +44,33 @@ struct ShotDevice {
   double* cost;                  // optional sum of 0.5*sp^2 (final esource)
 };
 
+// 2-D tensor maps of one shot's fields for the TMA kernels (box sizes in
+// stencil_tma.cu): vx/vz/px/pz/p with their stencil halos, and kappa.
+struct alignas(64) TmaMaps {
+  CUtensorMap vx19, vz72, px, pz, p72, vx16, vz16, kap;
+};
+
 struct FusedLaunch {
   const ShotDevice* shots;  // device array
   int nshots;
   int hist_fp16;
   int n1h;                  // history leading dimension
-  int chunk;                // columns per warp
+  int chunk;                // 0: TMA kernels; 1, 2, 4: columns per thread (register kernels)
   int max_rec, max_datum;   // largest station counts (gather CTAs)
+  const TmaMaps* maps;      // device array, one per shot (TMA kernels)
+  unsigned* err;            // raised by a bounded wait that ran out
+  int persist_p, persist_v; // persistent grid sizes of the TMA kernels
 };
+
+// TMA kernels (stencil_tma.cu)
+int tma_tiles(const Grid& g);
+void tma_prepare(int* persist_p, int* persist_v);
+void tma_p_step(const Grid& g, const ModelDev& m, const FusedLaunch& L, int mode, int it,
+                cudaStream_t st);
+void tma_v_step(const Grid& g, const ModelDev& m, const FusedLaunch& L, int mode, int it,
+                cudaStream_t st);
+bool tma_encode_maps(const Grid& g, const float* vx, const float* vz, const float* px,
+                     const float* pz, const float* p, const float* kap, TmaMaps* out);
 
 // Stage-A flush at it = nt+1 is folded into fused_p_step (it may exceed a
 // shot's nt by one in stage A).

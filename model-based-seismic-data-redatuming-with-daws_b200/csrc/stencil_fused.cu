@@ -164,7 +164,8 @@ __global__ void __launch_bounds__(kThreads)
   const size_t nih = (size_t)n1h * g.n2;
   const int i1 = t.i1;  // rows i1, i1+1
   const bool ok0 = i1 < n1e, ok1 = i1 + 1 < n1e;
-  const bool u0 = ok0 && i1 >= 2 && i1 < hi1, u1 = ok1 && i1 + 1 < hi1;  // i1 even: i1+1 >= 3
+  // update range [2, hi1) of each row (row 1 of the first lane is outside it)
+  const bool u0 = ok0 && i1 >= 2 && i1 < hi1, u1 = ok1 && i1 + 1 >= 2 && i1 + 1 < hi1;
   const bool r0 = ok0 && i1 >= npml && i1 < npml + g.n1;
   const bool r1 = ok1 && i1 + 1 >= npml && i1 + 1 < npml + g.n1;
   const int h1 = i1 - npml + (npml & 1);  // history row of i1 (even)
@@ -369,7 +370,7 @@ __global__ void __launch_bounds__(kThreads)
   const size_t nih = (size_t)n1h * g.n2;
   const int i1 = t.i1;
   const bool ok0 = i1 < n1e, ok1 = i1 + 1 < n1e;
-  const bool u0 = ok0 && i1 >= 2 && i1 < hi1, u1 = ok1 && i1 + 1 < hi1;
+  const bool u0 = ok0 && i1 >= 2 && i1 < hi1, u1 = ok1 && i1 + 1 >= 2 && i1 + 1 < hi1;
   const bool r0 = ok0 && i1 >= npml && i1 < npml + g.n1;
   const bool r1 = ok1 && i1 + 1 >= npml && i1 + 1 < npml + g.n1;
   const int h1 = i1 - npml + (npml & 1);

@@ -1,0 +1,706 @@
+// TMA-pipelined persistent time-step kernels (the default fused path).
+//
+// A persistent CTA (256 threads) walks tiles of 64 depth rows x 16 columns.
+// For every tile one thread issues 2-D tensor copies (cp.async.bulk.tensor)
+// of the fields the tile needs -- with their stencil halos -- into a
+// double-buffered shared-memory stage and arms an mbarrier with the byte
+// count; while the CTA computes tile k from stage k&1, the copies of tile
+// k+1 are in flight.  The copies zero-fill outside the grid, which supplies
+// the boundary values the stencil reads.  Each thread computes 2 rows x 2
+// columns from shared memory (conflict-free float2 reads) with the
+// reference's separately rounded FP32 operations, and writes its results
+// with coalesced float2 stores.
+//
+// Every mbarrier wait is bounded (clock64 budget, ~1 s); on expiry the
+// kernel raises the error flag and continues without hanging.
+#include <cuda.h>
+
+#include "fused.cuh"
+
+namespace daw {
+namespace {
+
+constexpr int TR = 64;        // rows per tile
+constexpr int TC = 16;        // columns per tile
+constexpr int HR = 4;         // row halo (16-byte aligned TMA start)
+constexpr int kThreadsT = 256;
+constexpr unsigned kAll = 0xffffffffu;
+
+// stage layouts (bytes, 128-aligned sections)
+constexpr int kPVX = TR * (TC + 3) * 4;       // 4864  vx, columns c0-2..c0+TC
+constexpr int kPVZ = (TR + 2 * HR) * TC * 4;  // 4608  vz, rows r0-4..r0+TR+3
+constexpr int kPF = TR * TC * 4;              // 4096  px, pz, kappa
+constexpr int kPStage = kPVX + kPVZ + 3 * kPF;  // 21760
+constexpr int kVP = 5504;                     // p, 72 rows x 19 columns (5472, padded)
+constexpr int kVStage = kVP + 2 * kPF;        // 13696
+constexpr int kGatherBytes = 8 * 444 * 4;     // 14208
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void bar_init(uint64_t* b) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(b)), "r"(1) : "memory");
+}
+__device__ __forceinline__ void bar_expect(uint64_t* b, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(b)),
+               "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ bool bar_try(uint64_t* b, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+      " selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(b)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Bounded wait: ~2^31 cycles, then the error flag is raised and the caller
+// proceeds (results of that launch are then invalid; the host reports it).
+__device__ __forceinline__ void bar_wait(uint64_t* b, uint32_t parity, unsigned* err) {
+  if (bar_try(b, parity)) return;
+  const long long t0 = clock64();
+  while (!bar_try(b, parity)) {
+    if (clock64() - t0 > (1LL << 31)) {
+      atomicOr(err, 1u);
+      return;
+    }
+  }
+}
+__device__ __forceinline__ void tma_2d(void* dst, const CUtensorMap* map, int x, int y,
+                                       uint64_t* b) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3}], [%4];" ::"r"(smem_u32(dst)),
+      "l"(map), "r"(x), "r"(y), "r"(smem_u32(b))
+      : "memory");
+}
+
+__device__ __forceinline__ int amax_exponent(unsigned bits) {
+  const int ef = (int)(bits >> 23);
+  const int e = (ef == 0) ? -126 : ef - 126;
+  return max(min(e, 120), -100);
+}
+__device__ __forceinline__ float pow2f(int e) { return __int_as_float((e + 127) << 23); }
+__device__ __forceinline__ unsigned warp_amax_slots(const unsigned* slots) {
+  return __reduce_max_sync(kAll, slots[threadIdx.x & 31]);
+}
+__device__ __forceinline__ void warp_amax_flush(float v, unsigned* slot) {
+  const unsigned b = __reduce_max_sync(kAll, __float_as_uint(v));
+  if ((threadIdx.x & 31) == 0 && b) atomicMax(slot, b);
+}
+
+template <bool FP16>
+struct Hist;
+template <>
+struct Hist<true> {
+  static __device__ __forceinline__ void put2(void* base, int o, float a, float b, float inv,
+                                              bool v0, bool v1) {
+    __half* h = static_cast<__half*>(base);
+    if (v0 && v1)
+      *reinterpret_cast<__half2*>(h + o) = __floats2half2_rn(a * inv, b * inv);
+    else if (v0)
+      h[o] = __float2half_rn(a * inv);
+    else if (v1)
+      h[o + 1] = __float2half_rn(b * inv);
+  }
+  static __device__ __forceinline__ float2 get2(const void* base, int o, float sc, bool v0,
+                                                bool v1) {
+    const __half* h = static_cast<const __half*>(base);
+    if (v0 && v1) {
+      const float2 f = __half22float2(*reinterpret_cast<const __half2*>(h + o));
+      return make_float2(f.x * sc, f.y * sc);
+    }
+    return make_float2(v0 ? __half2float(h[o]) * sc : 0.f, v1 ? __half2float(h[o + 1]) * sc : 0.f);
+  }
+};
+template <>
+struct Hist<false> {
+  static __device__ __forceinline__ void put2(void* base, int o, float a, float b, float,
+                                              bool v0, bool v1) {
+    float* h = static_cast<float*>(base);
+    if (v0 && v1)
+      *reinterpret_cast<float2*>(h + o) = make_float2(a, b);
+    else if (v0)
+      h[o] = a;
+    else if (v1)
+      h[o + 1] = b;
+  }
+  static __device__ __forceinline__ float2 get2(const void* base, int o, float, bool v0,
+                                                bool v1) {
+    const float* h = static_cast<const float*>(base);
+    if (v0 && v1) return *reinterpret_cast<const float2*>(h + o);
+    return make_float2(v0 ? h[o] : 0.f, v1 ? h[o + 1] : 0.f);
+  }
+};
+
+template <bool FP16>
+__device__ __forceinline__ void* step_ptr(void* hist, int step0, size_t nih) {
+  return static_cast<char*>(hist) + (size_t)step0 * 3 * nih * (FP16 ? 2 : 4);
+}
+
+__device__ __forceinline__ float inject_at(const InjMapDev& m, float v, int i1, int clo, int base,
+                                           float dt, float w, const float* amp, int amp_stride,
+                                           int sign) {
+  const int r = base + (i1 - clo);
+  const int e0 = __ldg(m.rowptr + 2 * r), e1 = __ldg(m.rowptr + 2 * r + 1);
+  for (int e = e0; e < e1; ++e) {
+    const float a = __ldg(amp + (size_t)__ldg(m.sta + e) * amp_stride);
+    const float term = fmul(fmul(fmul(__ldg(m.coef + e), dt), a), w);
+    v = sign > 0 ? fadd(v, term) : fsub(v, term);
+  }
+  return v;
+}
+
+struct TileId {
+  int shot, r0, c0;
+};
+
+__device__ __forceinline__ TileId tile_id(const Grid& g, int t) {
+  const int nrb = (g.n1e + TR - 1) / TR, ncb = (g.n2e + TC - 1) / TC;
+  const int tps = nrb * ncb;
+  TileId id;
+  id.shot = t / tps;
+  const int l = t - id.shot * tps;
+  id.r0 = (l % nrb) * TR;
+  id.c0 = (l / nrb) * TC;
+  return id;
+}
+
+// ---------------------------------------------------------------------------
+// Pressure kernel
+// ---------------------------------------------------------------------------
+template <int MODE, bool FP16>
+__global__ void __launch_bounds__(kThreadsT)
+    k_tma_p(const Grid g, const ModelDev m, const FusedLaunch L, const int it, const int ntiles) {
+  using H = Hist<FP16>;
+  extern __shared__ __align__(128) unsigned char smem[];
+  uint64_t* bar = reinterpret_cast<uint64_t*>(smem + 2 * kPStage);
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  if (tid == 0) {
+    bar_init(&bar[0]);
+    bar_init(&bar[1]);
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  }
+  __syncthreads();
+  auto issue = [&](int t, int s) {
+    const TileId id = tile_id(g, t);
+    const TmaMaps* mp = L.maps + id.shot;
+    unsigned char* st = smem + s * kPStage;
+    bar_expect(&bar[s], kPStage);
+    tma_2d(st, &mp->vx19, id.r0, id.c0 - 2, &bar[s]);
+    tma_2d(st + kPVX, &mp->vz72, id.r0 - HR, id.c0, &bar[s]);
+    tma_2d(st + kPVX + kPVZ, &mp->px, id.r0, id.c0, &bar[s]);
+    tma_2d(st + kPVX + kPVZ + kPF, &mp->pz, id.r0, id.c0, &bar[s]);
+    tma_2d(st + kPVX + kPVZ + 2 * kPF, &mp->kap, id.r0, id.c0, &bar[s]);
+  };
+  int t = blockIdx.x;
+  if (tid == 0 && t < ntiles) issue(t, 0);
+  uint32_t phase0 = 0, phase1 = 0;
+  int stage = 0;
+  int cur_shot = -1;
+  float lmax = 0.f;
+  const int ld = g.ld, n1e = g.n1e, n2e = g.n2e, npml = g.npml;
+  const int off = (MODE == FM_FWD) ? 2 : 3;
+  const int hi1 = n1e - off, hi2 = n2e - off;
+  const int fsrows = g.ofs == 1 ? npml + 1 : 0;
+  const int n1h = L.n1h;
+  const size_t nih = (size_t)n1h * g.n2;
+  const float dtdx = g.dtdx, dt = g.dt, mdt = fmul(-1.0f, dt);
+  for (; t < ntiles; t += gridDim.x) {
+    const int tn = t + gridDim.x;
+    if (tid == 0 && tn < ntiles) issue(tn, stage ^ 1);
+    const TileId id = tile_id(g, t);
+    const ShotDevice sd = L.shots[id.shot];
+    if (MODE == FM_STAGE_A && id.shot != cur_shot) {
+      if (cur_shot >= 0) {
+        const ShotDevice& so = L.shots[cur_shot];
+        warp_amax_flush(lmax, so.amax + (size_t)(it - 1) * 3 * kAmaxSlots +
+                                  ((blockIdx.x * 8 + warp) % kAmaxSlots));
+      }
+      cur_shot = id.shot;
+      lmax = 0.f;
+    }
+    const int nt = sd.nt;
+    const bool live = sd.active && (MODE == FM_STAGE_A ? it <= nt + 1 : it <= nt);
+    const bool flush = (MODE == FM_STAGE_A) && it == nt + 1;
+    const int ic = nt - it + 1;
+    const int i1 = id.r0 + 2 * lane;
+    const bool ok0 = i1 < n1e, ok1 = i1 + 1 < n1e;
+    const bool u0 = ok0 && i1 >= 2 && i1 < hi1, u1 = ok1 && i1 + 1 >= 2 && i1 + 1 < hi1;
+    const bool r0 = ok0 && i1 >= npml && i1 < npml + g.n1;
+    const bool r1 = ok1 && i1 + 1 >= npml && i1 + 1 < npml + g.n1;
+    const int h1 = i1 - npml + (npml & 1);
+    // stage-B history (HBM stream) issued before waiting on the tile
+    float sc_p = 1.f, inv_vx = 1.f, inv_vz = 1.f;
+    float2 hv[2] = {make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
+    const int slo = (MODE == FM_STAGE_B_ES) ? 1 : 0;
+    const int shi1 = (MODE == FM_STAGE_B_ES) ? g.n1 - 1 : g.n1;
+    const int shi2 = (MODE == FM_STAGE_B_ES) ? g.n2 - 1 : g.n2;
+    const bool s0 = r0 && i1 - npml >= slo && i1 - npml < shi1;
+    const bool s1 = r1 && i1 + 1 - npml >= slo && i1 + 1 - npml < shi1;
+    if (live && (MODE == FM_STAGE_B || MODE == FM_STAGE_B_ES)) {
+      if (FP16) sc_p = pow2f(amax_exponent(warp_amax_slots(sd.amax + (size_t)(ic - 1) * 3 * kAmaxSlots)) - 15);
+      const void* hp = step_ptr<FP16>(sd.hist, ic - 1, nih);
+#pragma unroll
+      for (int j = 0; j < 2; ++j) {
+        const int c = id.c0 + 2 * warp + j;
+        const int i2p = c - npml;
+        if (c < n2e && i2p >= slo && i2p < shi2 && (s0 || s1))
+          hv[j] = H::get2(hp, h1 + n1h * i2p, sc_p, s0, s1);
+      }
+    }
+    if (live && FP16 && MODE == FM_STAGE_A && it >= 2) {
+      const unsigned* a = sd.amax + (size_t)(it - 2) * 3 * kAmaxSlots;
+      inv_vx = pow2f(15 - amax_exponent(warp_amax_slots(a + kAmaxSlots)));
+      inv_vz = pow2f(15 - amax_exponent(warp_amax_slots(a + 2 * kAmaxSlots)));
+    }
+    bar_wait(&bar[stage], stage ? phase1 : phase0, L.err);
+    if (stage) phase1 ^= 1; else phase0 ^= 1;
+    const unsigned char* st = smem + stage * kPStage;
+    const float2* VX = reinterpret_cast<const float2*>(st);              // [TC+3][32]
+    const float* VZ = reinterpret_cast<const float*>(st + kPVX);         // [TC][72]
+    const float2* PX = reinterpret_cast<const float2*>(st + kPVX + kPVZ);
+    const float2* PZ = PX + TR * TC / 2;
+    const float2* KA = PZ + TR * TC / 2;
+    if (live) {
+      void* hvs = (MODE == FM_STAGE_A && it >= 2) ? step_ptr<FP16>(sd.hist, it - 2, nih) : nullptr;
+      const bool do_inj = (MODE == FM_STAGE_A) || (MODE == FM_FWD && sd.type_src == 0);
+      const float2 d1a = ok1 ? __ldg(reinterpret_cast<const float2*>(m.d1a + i1))
+                             : make_float2(ok0 ? __ldg(m.d1a + i1) : 0.f, 0.f);
+      const float2 d1a1 = ok1 ? __ldg(reinterpret_cast<const float2*>(m.d1a1 + i1))
+                              : make_float2(ok0 ? __ldg(m.d1a1 + i1) : 0.f, 0.f);
+#pragma unroll
+      for (int j = 0; j < 2; ++j) {
+        const int cc = 2 * warp + j;
+        const int c = id.c0 + cc;
+        if (c >= n2e || !ok0) continue;
+        const int k = i1 + ld * c;
+        const float2 q0 = VX[(cc + 0) * 32 + lane], q1 = VX[(cc + 1) * 32 + lane];
+        const float2 q2 = VX[(cc + 2) * 32 + lane], q3 = VX[(cc + 3) * 32 + lane];
+        const float* vzc = VZ + cc * (TR + 2 * HR) + 2 * lane;  // row r0+2l-4
+        const float2 zm = *reinterpret_cast<const float2*>(vzc + 2);  // rows i1-2, i1-1
+        const float2 z = *reinterpret_cast<const float2*>(vzc + 4);   // rows i1, i1+1
+        const float zp2 = vzc[6];                                     // row i1+2
+        const int i2p = c - npml;
+        const bool cint = i2p >= 0 && i2p < g.n2;
+        if (MODE == FM_STAGE_A && it >= 2 && cint && (r0 || r1)) {
+          const int ho = h1 + n1h * i2p;
+          H::put2(hvs, (int)nih + ho, q2.x, q2.y, inv_vx, r0, r1);
+          H::put2(hvs, 2 * (int)nih + ho, z.x, z.y, inv_vz, r0, r1);
+        }
+        if (flush) continue;
+        float2 px_ = PX[cc * 32 + lane], pz_ = PZ[cc * 32 + lane];
+        const float2 kv = KA[cc * 32 + lane];
+        if (c >= 2 && c < hi2) {
+          const float kw2f = __ldg(m.d2a1 + c), d2a = __ldg(m.d2a + c);
+          const bool fwd = (MODE != FM_STAGE_A);
+          if (u0) {
+            const float der2 = dminus(q0.x, q1.x, q2.x, q3.x);
+            const float der1 = dminus(zm.x, zm.y, z.x, z.y);
+            const float kd = fmul(dtdx, kv.x);
+            const float ax = fmul(d2a, px_.x), bx = fmul(fmul(kd, kw2f), der2);
+            const float az = fmul(d1a.x, pz_.x), bz = fmul(fmul(kd, d1a1.x), der1);
+            px_.x = fwd ? fadd(ax, bx) : fsub(ax, bx);
+            pz_.x = fwd ? fadd(az, bz) : fsub(az, bz);
+          }
+          if (u1) {
+            const float der2 = dminus(q0.y, q1.y, q2.y, q3.y);
+            const float der1 = dminus(zm.y, z.x, z.y, zp2);
+            const float kd = fmul(dtdx, kv.y);
+            const float ax = fmul(d2a, px_.y), bx = fmul(fmul(kd, kw2f), der2);
+            const float az = fmul(d1a.y, pz_.y), bz = fmul(fmul(kd, d1a1.y), der1);
+            px_.y = fwd ? fadd(ax, bx) : fsub(ax, bx);
+            pz_.y = fwd ? fadd(az, bz) : fsub(az, bz);
+          }
+        }
+        if (do_inj) {
+          const int clo = __ldg(sd.inj.col_lo + c);
+          const int chi = __ldg(sd.inj.col_hi + c);
+          if (i1 + 1 >= clo && i1 <= chi) {
+            const int base = __ldg(sd.inj.col_base + c);
+            const int sg = MODE == FM_FWD ? +1 : -1;
+            if (i1 >= clo && i1 <= chi)
+              px_.x = inject_at(sd.inj, px_.x, i1, clo, base, dt, kv.x, sd.amp + (it - 1),
+                                sd.amp_stride, sg);
+            if (ok1 && i1 + 1 >= clo && i1 + 1 <= chi)
+              px_.y = inject_at(sd.inj, px_.y, i1 + 1, clo, base, dt, kv.y, sd.amp + (it - 1),
+                                sd.amp_stride, sg);
+          }
+        }
+        if (MODE == FM_STAGE_B || MODE == FM_STAGE_B_ES) {
+          if (i2p >= slo && i2p < shi2) {
+            if (s0) px_.x = fadd(px_.x, fmul(fmul(mdt, hv[j].x), kv.x));
+            if (s1) px_.y = fadd(px_.y, fmul(fmul(mdt, hv[j].y), kv.y));
+          }
+        }
+        float2 pv;
+        pv.x = i1 < fsrows ? 0.f : fadd(px_.x, pz_.x);
+        pv.y = i1 + 1 < fsrows ? 0.f : fadd(px_.y, pz_.y);
+        *reinterpret_cast<float2*>(sd.px + k) = px_;
+        *reinterpret_cast<float2*>(sd.pz + k) = pz_;
+        *reinterpret_cast<float2*>(sd.p + k) = pv;
+        if (cint) {
+          if (MODE == FM_STAGE_A) {
+            if (r0) lmax = fmaxf(lmax, fabsf(pv.x));
+            if (r1) lmax = fmaxf(lmax, fabsf(pv.y));
+          }
+          if ((MODE == FM_FWD || MODE == FM_STAGE_B_ES) && sd.wf && sd.type_rec == 0) {
+            float* w = sd.wf + (size_t)(it - 1) * g.int_elems() + (size_t)g.n1 * i2p;
+            const int i1p = i1 - npml;
+            if (MODE == FM_FWD) {
+              if (r0) w[i1p] = pv.x;
+              if (r1) w[i1p + 1] = pv.y;
+            } else {
+              if (r0) w[i1p] = fadd(w[i1p], pv.x);
+              if (r1) w[i1p + 1] = fadd(w[i1p + 1], pv.y);
+            }
+          }
+        }
+      }
+    }
+    __syncthreads();  // stage buffer free for the copy issued next iteration
+    stage ^= 1;
+  }
+  if (MODE == FM_STAGE_A && cur_shot >= 0) {
+    const ShotDevice& so = L.shots[cur_shot];
+    warp_amax_flush(lmax, so.amax + (size_t)(it - 1) * 3 * kAmaxSlots +
+                              ((blockIdx.x * 8 + warp) % kAmaxSlots));
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Velocity kernel; gather tiles (8 stations each) come first.
+// ---------------------------------------------------------------------------
+template <int MODE, bool FP16>
+__global__ void __launch_bounds__(kThreadsT)
+    k_tma_v(const Grid g, const ModelDev m, const FusedLaunch L, const int it, const int ntiles,
+            const int ngb_per_shot) {
+  using H = Hist<FP16>;
+  extern __shared__ __align__(128) unsigned char smem[];
+  uint64_t* bar = reinterpret_cast<uint64_t*>(smem + 2 * kVStage);
+  float* prod = reinterpret_cast<float*>(smem + 2 * kVStage + 128);
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  if (tid == 0) {
+    bar_init(&bar[0]);
+    bar_init(&bar[1]);
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  }
+  __syncthreads();
+  auto issue = [&](int t, int s) {
+    const TileId id = tile_id(g, t);
+    const TmaMaps* mp = L.maps + id.shot;
+    unsigned char* st = smem + s * kVStage;
+    bar_expect(&bar[s], TR * (TC + 3) * 4 + HR * 2 * (TC + 3) * 4 + 2 * kPF);
+    tma_2d(st, &mp->p72, id.r0 - HR, id.c0 - 1, &bar[s]);
+    tma_2d(st + kVP, &mp->vx16, id.r0, id.c0, &bar[s]);
+    tma_2d(st + kVP + kPF, &mp->vz16, id.r0, id.c0, &bar[s]);
+  };
+  int t = blockIdx.x;
+  if (tid == 0 && t < ntiles) issue(t, 0);
+  // gathers while the first tile is in flight
+  if (MODE != FM_STAGE_A) {
+    const int ngb = ngb_per_shot * L.nshots;
+    for (int gb = blockIdx.x; gb < ngb; gb += gridDim.x) {
+      const int shot = gb / ngb_per_shot;
+      const ShotDevice& sd = L.shots[shot];
+      if (!sd.active || it > sd.nt || sd.type_rec != 0) continue;
+      const int s = (gb % ngb_per_shot) * 8 + warp;
+      if (s < sd.rec.n) {
+        if (sd.out) {
+          const float v = warp_gather_ordered(prod + warp * 444, sd.rec.ix1, sd.rec.ix2,
+                                              sd.rec.tile, s, sd.p, g.ld, 0, g.n1e, g.n2e);
+          const int row = sd.out_reverse ? sd.nt - it : it - 1;
+          if (lane == 0) sd.out[row + (size_t)sd.nt * s] = v;
+        }
+      } else if (s - sd.rec.n < sd.datum.n && sd.red &&
+                 (MODE == FM_FWD || MODE == FM_STAGE_B_ES)) {
+        const int d = s - sd.rec.n;
+        const float v = warp_gather_ordered(prod + warp * 444, sd.datum.ix1, sd.datum.ix2,
+                                            sd.datum.tile, d,
+                                            sd.p + g.npml + (size_t)g.ld * g.npml, g.ld,
+                                            g.npml, g.n1, g.n2);
+        if (lane == 0) sd.red[(it - 1) + (size_t)sd.nt * d] = v;
+      }
+    }
+  }
+  uint32_t phase0 = 0, phase1 = 0;
+  int stage = 0;
+  int cur_shot = -1;
+  float lmx = 0.f, lmz = 0.f;
+  const int ld = g.ld, n1e = g.n1e, n2e = g.n2e, npml = g.npml;
+  const int off = (MODE == FM_FWD) ? 2 : 3;
+  const int hi1 = n1e - off, hi2 = n2e - off;
+  const int n1h = L.n1h;
+  const size_t nih = (size_t)n1h * g.n2;
+  const float dt = g.dt, mdt = fmul(-1.0f, dt);
+  const bool fs = g.ofs == 1;
+  for (; t < ntiles; t += gridDim.x) {
+    const int tn = t + gridDim.x;
+    if (tid == 0 && tn < ntiles) issue(tn, stage ^ 1);
+    const TileId id = tile_id(g, t);
+    const ShotDevice sd = L.shots[id.shot];
+    if (MODE == FM_STAGE_A && id.shot != cur_shot) {
+      if (cur_shot >= 0) {
+        unsigned* a = L.shots[cur_shot].amax + (size_t)(it - 1) * 3 * kAmaxSlots +
+                      ((blockIdx.x * 8 + warp) % kAmaxSlots);
+        warp_amax_flush(lmx, a + kAmaxSlots);
+        warp_amax_flush(lmz, a + 2 * kAmaxSlots);
+      }
+      cur_shot = id.shot;
+      lmx = lmz = 0.f;
+    }
+    const int nt = sd.nt;
+    const bool live = sd.active && it <= nt;
+    const int ic = nt - it + 1;
+    const int i1 = id.r0 + 2 * lane;
+    const bool ok0 = i1 < n1e, ok1 = i1 + 1 < n1e;
+    const bool u0 = ok0 && i1 >= 2 && i1 < hi1, u1 = ok1 && i1 + 1 >= 2 && i1 + 1 < hi1;
+    const bool r0 = ok0 && i1 >= npml && i1 < npml + g.n1;
+    const bool r1 = ok1 && i1 + 1 >= npml && i1 + 1 < npml + g.n1;
+    const int h1 = i1 - npml + (npml & 1);
+    float inv_p = 1.f;
+    float2 hx[2] = {make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
+    float2 hz[2] = {make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
+    if (live && (MODE == FM_STAGE_B || MODE == FM_STAGE_B_ES)) {
+      float sc_vx = 1.f, sc_vz = 1.f;
+      if (FP16) {
+        const unsigned* a = sd.amax + (size_t)(ic - 1) * 3 * kAmaxSlots;
+        sc_vx = pow2f(amax_exponent(warp_amax_slots(a + kAmaxSlots)) - 15);
+        sc_vz = pow2f(amax_exponent(warp_amax_slots(a + 2 * kAmaxSlots)) - 15);
+      }
+      const void* hp = step_ptr<FP16>(sd.hist, ic - 1, nih);
+#pragma unroll
+      for (int j = 0; j < 2; ++j) {
+        const int c = id.c0 + 2 * warp + j;
+        const int i2p = c - npml;
+        if (c < n2e && i2p >= 0 && i2p < g.n2 && (r0 || r1)) {
+          const int ho = h1 + n1h * i2p;
+          hx[j] = H::get2(hp, (int)nih + ho, sc_vx, r0, r1);
+          hz[j] = H::get2(hp, 2 * (int)nih + ho, sc_vz, r0, r1);
+        }
+      }
+    }
+    if (live && FP16 && MODE == FM_STAGE_A)
+      inv_p = pow2f(15 - amax_exponent(warp_amax_slots(sd.amax + (size_t)(it - 1) * 3 * kAmaxSlots)));
+    bar_wait(&bar[stage], stage ? phase1 : phase0, L.err);
+    if (stage) phase1 ^= 1; else phase0 ^= 1;
+    const unsigned char* st = smem + stage * kVStage;
+    const float* P = reinterpret_cast<const float*>(st);  // [TC+3][72], row 0 = r0-4, col 0 = c0-1
+    const float2* VX = reinterpret_cast<const float2*>(st + kVP);
+    const float2* VZ = VX + TR * TC / 2;
+    if (live) {
+      void* hps = (MODE == FM_STAGE_A) ? step_ptr<FP16>(sd.hist, it - 1, nih) : nullptr;
+      const bool do_inj = (MODE == FM_FWD) && sd.type_src == 1;
+      const float2 d1b = ok1 ? __ldg(reinterpret_cast<const float2*>(m.d1b + i1))
+                             : make_float2(ok0 ? __ldg(m.d1b + i1) : 0.f, 0.f);
+      const float2 bw1 = ok1 ? __ldg(reinterpret_cast<const float2*>(m.bw1 + i1))
+                             : make_float2(ok0 ? __ldg(m.bw1 + i1) : 0.f, 0.f);
+      const bool dst_x = fs && i1 == npml - 1;
+      const bool skip_y = fs && i1 + 1 == npml - 1;
+      const bool src_x = fs && i1 == npml;
+#pragma unroll
+      for (int j = 0; j < 2; ++j) {
+        const int cc = 2 * warp + j;
+        const int c = id.c0 + cc;
+        if (c >= n2e || !ok0) continue;
+        const int k = i1 + ld * c;
+        const float* pcol = P + (cc + 1) * (TR + 2 * HR) + 2 * lane;  // own column, row r0+2l-4
+        const float pm1 = pcol[3];                                           // row i1-1
+        const float2 pc = *reinterpret_cast<const float2*>(pcol + 4);        // rows i1, i1+1
+        const float2 pp = *reinterpret_cast<const float2*>(pcol + 6);        // rows i1+2, i1+3
+        const float2 a0 = *reinterpret_cast<const float2*>(P + cc * (TR + 2 * HR) + 2 * lane + 4);
+        const float2 a2 = *reinterpret_cast<const float2*>(P + (cc + 2) * (TR + 2 * HR) + 2 * lane + 4);
+        const float2 a3 = *reinterpret_cast<const float2*>(P + (cc + 3) * (TR + 2 * HR) + 2 * lane + 4);
+        const int i2p = c - npml;
+        const bool cint = i2p >= 0 && i2p < g.n2;
+        float2 vx_ = VX[cc * 32 + lane], vz_ = VZ[cc * 32 + lane];
+        if (c >= 2 && c < hi2) {
+          const float d2b = __ldg(m.d2b + c), bw2 = __ldg(m.bw2 + c);
+          const bool fwd = (MODE != FM_STAGE_A);
+          if (u0) {
+            const float der2 = dplus(a0.x, pc.x, a2.x, a3.x);
+            const float der1 = dplus(pm1, pc.x, pc.y, pp.x);
+            const float ax = fmul(d2b, vx_.x), bx = fmul(bw2, der2);
+            const float az = fmul(d1b.x, vz_.x), bz = fmul(bw1.x, der1);
+            vx_.x = fwd ? fadd(ax, bx) : fsub(ax, bx);
+            vz_.x = fwd ? fadd(az, bz) : fsub(az, bz);
+          }
+          if (u1) {
+            const float der2 = dplus(a0.y, pc.y, a2.y, a3.y);
+            const float der1 = dplus(pc.x, pc.y, pp.x, pp.y);
+            const float ax = fmul(d2b, vx_.y), bx = fmul(bw2, der2);
+            const float az = fmul(d1b.y, vz_.y), bz = fmul(bw1.y, der1);
+            vx_.y = fwd ? fadd(ax, bx) : fsub(ax, bx);
+            vz_.y = fwd ? fadd(az, bz) : fsub(az, bz);
+          }
+        }
+        if ((MODE == FM_STAGE_B || MODE == FM_STAGE_B_ES) && cint) {
+          if (r0) {
+            vx_.x = fadd(vx_.x, fmul(fmul(mdt, hx[j].x), 1.0f));
+            vz_.x = fadd(vz_.x, fmul(fmul(mdt, hz[j].x), 1.0f));
+          }
+          if (r1) {
+            vx_.y = fadd(vx_.y, fmul(fmul(mdt, hx[j].y), 1.0f));
+            vz_.y = fadd(vz_.y, fmul(fmul(mdt, hz[j].y), 1.0f));
+          }
+        }
+        if (do_inj) {
+          const int clo = __ldg(sd.inj.col_lo + c);
+          const int chi = __ldg(sd.inj.col_hi + c);
+          if (i1 + 1 >= clo && i1 <= chi) {
+            const int base = __ldg(sd.inj.col_base + c);
+            if (i1 >= clo && i1 <= chi)
+              vz_.x = inject_at(sd.inj, vz_.x, i1, clo, base, dt, 1.0f, sd.amp + (it - 1),
+                                sd.amp_stride, +1);
+            if (ok1 && i1 + 1 >= clo && i1 + 1 <= chi)
+              vz_.y = inject_at(sd.inj, vz_.y, i1 + 1, clo, base, dt, 1.0f, sd.amp + (it - 1),
+                                sd.amp_stride, +1);
+          }
+        }
+        if (dst_x) vz_.x = vz_.y;
+        *reinterpret_cast<float2*>(sd.vx + k) = vx_;
+        if (skip_y)
+          sd.vz[k] = vz_.x;
+        else
+          *reinterpret_cast<float2*>(sd.vz + k) = vz_;
+        if (src_x) sd.vz[k - 1] = vz_.x;
+        if (MODE == FM_STAGE_A && cint && (r0 || r1)) {
+          H::put2(hps, h1 + n1h * i2p, pc.x, pc.y, inv_p, r0, r1);
+          if (r0) {
+            lmx = fmaxf(lmx, fabsf(vx_.x));
+            lmz = fmaxf(lmz, fabsf(vz_.x));
+          }
+          if (r1) {
+            lmx = fmaxf(lmx, fabsf(vx_.y));
+            lmz = fmaxf(lmz, fabsf(vz_.y));
+          }
+        }
+      }
+    }
+    __syncthreads();
+    stage ^= 1;
+  }
+  if (MODE == FM_STAGE_A && cur_shot >= 0) {
+    unsigned* a = L.shots[cur_shot].amax + (size_t)(it - 1) * 3 * kAmaxSlots +
+                  ((blockIdx.x * 8 + warp) % kAmaxSlots);
+    warp_amax_flush(lmx, a + kAmaxSlots);
+    warp_amax_flush(lmz, a + 2 * kAmaxSlots);
+  }
+}
+
+template <int MODE>
+void launch_p(const Grid& g, const ModelDev& m, const FusedLaunch& L, int it, cudaStream_t st) {
+  const int ntiles = tma_tiles(g) * L.nshots;
+  const int grid = std::min(ntiles, L.persist_p);
+  const size_t smem = 2 * kPStage + 16;
+  if (L.hist_fp16)
+    k_tma_p<MODE, true><<<grid, kThreadsT, smem, st>>>(g, m, L, it, ntiles);
+  else
+    k_tma_p<MODE, false><<<grid, kThreadsT, smem, st>>>(g, m, L, it, ntiles);
+}
+
+template <int MODE>
+void launch_v(const Grid& g, const ModelDev& m, const FusedLaunch& L, int it, cudaStream_t st) {
+  const int ntiles = tma_tiles(g) * L.nshots;
+  const int stations = (MODE == FM_STAGE_A) ? 0 : L.max_rec + L.max_datum;
+  const int ngbps = (stations + 7) / 8;
+  const int grid = std::max(1, std::min(std::max(ntiles, ngbps * L.nshots), L.persist_v));
+  const size_t smem = 2 * kVStage + 128 + kGatherBytes;
+  if (L.hist_fp16)
+    k_tma_v<MODE, true><<<grid, kThreadsT, smem, st>>>(g, m, L, it, ntiles, ngbps);
+  else
+    k_tma_v<MODE, false><<<grid, kThreadsT, smem, st>>>(g, m, L, it, ntiles, ngbps);
+}
+
+template <typename K>
+int occupancy(K kernel, size_t smem) {
+  cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  int n = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel, kThreadsT, smem);
+  return n;
+}
+
+template <int MODE, bool FP16>
+void prep_mode(int* pp, int* pv) {
+  *pp = std::min(*pp, occupancy(k_tma_p<MODE, FP16>, 2 * kPStage + 16));
+  *pv = std::min(*pv, occupancy(k_tma_v<MODE, FP16>, 2 * kVStage + 128 + kGatherBytes));
+}
+
+}  // namespace
+
+int tma_tiles(const Grid& g) { return ((g.n1e + TR - 1) / TR) * ((g.n2e + TC - 1) / TC); }
+
+// Persistent grid sizes (CTAs resident on all SMs) and the dynamic shared
+// memory opt-in of every instantiation; call once per device, outside graph
+// capture.
+void tma_prepare(int* persist_p, int* persist_v) {
+  int dev = 0, sms = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  int op = 64, ov = 64;
+  prep_mode<FM_FWD, true>(&op, &ov);
+  prep_mode<FM_FWD, false>(&op, &ov);
+  prep_mode<FM_STAGE_A, true>(&op, &ov);
+  prep_mode<FM_STAGE_A, false>(&op, &ov);
+  prep_mode<FM_STAGE_B, true>(&op, &ov);
+  prep_mode<FM_STAGE_B, false>(&op, &ov);
+  prep_mode<FM_STAGE_B_ES, true>(&op, &ov);
+  prep_mode<FM_STAGE_B_ES, false>(&op, &ov);
+  *persist_p = std::max(1, op) * sms;
+  *persist_v = std::max(1, ov) * sms;
+}
+
+void tma_p_step(const Grid& g, const ModelDev& m, const FusedLaunch& L, int mode, int it,
+                cudaStream_t st) {
+  switch (mode) {
+    case FM_FWD: launch_p<FM_FWD>(g, m, L, it, st); break;
+    case FM_STAGE_A: launch_p<FM_STAGE_A>(g, m, L, it, st); break;
+    case FM_STAGE_B: launch_p<FM_STAGE_B>(g, m, L, it, st); break;
+    default: launch_p<FM_STAGE_B_ES>(g, m, L, it, st); break;
+  }
+}
+
+void tma_v_step(const Grid& g, const ModelDev& m, const FusedLaunch& L, int mode, int it,
+                cudaStream_t st) {
+  switch (mode) {
+    case FM_FWD: launch_v<FM_FWD>(g, m, L, it, st); break;
+    case FM_STAGE_A: launch_v<FM_STAGE_A>(g, m, L, it, st); break;
+    case FM_STAGE_B: launch_v<FM_STAGE_B>(g, m, L, it, st); break;
+    default: launch_v<FM_STAGE_B_ES>(g, m, L, it, st); break;
+  }
+}
+
+// Host: the eight 2-D tensor maps of one shot (extended-grid fields,
+// innermost dimension n1e rows with stride ld, n2e columns).
+bool tma_encode_maps(const Grid& g, const float* vx, const float* vz, const float* px,
+                     const float* pz, const float* p, const float* kap, TmaMaps* out) {
+  static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+  if (!encode) {
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", reinterpret_cast<void**>(&encode),
+                                cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess || !encode) {
+      encode = nullptr;
+      return false;
+    }
+  }
+  auto make = [&](CUtensorMap* map, const float* base, int br, int bc) {
+    cuuint64_t dims[2] = {(cuuint64_t)g.n1e, (cuuint64_t)g.n2e};
+    cuuint64_t strides[1] = {(cuuint64_t)g.ld * sizeof(float)};
+    cuuint32_t box[2] = {(cuuint32_t)br, (cuuint32_t)bc};
+    cuuint32_t es[2] = {1, 1};
+    return encode(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float*>(base), dims,
+                  strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                  CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) ==
+           CUDA_SUCCESS;
+  };
+  return make(&out->vx19, vx, TR, TC + 3) && make(&out->vz72, vz, TR + 2 * HR, TC) &&
+         make(&out->px, px, TR, TC) && make(&out->pz, pz, TR, TC) &&
+         make(&out->p72, p, TR + 2 * HR, TC + 3) && make(&out->vx16, vx, TR, TC) &&
+         make(&out->vz16, vz, TR, TC) && make(&out->kap, kap, TR, TC);
+}
+
+}  // namespace daw
