@@ -1,15 +1,21 @@
 // TMA-pipelined persistent time-step kernels (the default fused path).
 //
-// A persistent CTA (256 threads) walks tiles of 64 depth rows x 16 columns.
+// A persistent CTA (256 threads) walks tiles of 64 depth rows x 32 columns.
 // For every tile one thread issues 2-D tensor copies (cp.async.bulk.tensor)
 // of the fields the tile needs -- with their stencil halos -- into a
 // double-buffered shared-memory stage and arms an mbarrier with the byte
 // count; while the CTA computes tile k from stage k&1, the copies of tile
 // k+1 are in flight.  The copies zero-fill outside the grid, which supplies
-// the boundary values the stencil reads.  Each thread computes 2 rows x 2
+// the boundary values the stencil reads.  Each thread computes 2 rows x 4
 // columns from shared memory (conflict-free float2 reads) with the
 // reference's separately rounded FP32 operations, and writes its results
 // with coalesced float2 stores.
+//
+// Everything else a tile needs from global memory (the stage-B history
+// stream, the 1-D sponge profiles, the injection bands) is loaded into
+// registers before the CTA waits for the tile, so those latencies overlap the
+// copy; the shot descriptor and the step's FP16 scales are fetched once per
+// shot, not per tile.
 //
 // Every mbarrier wait is bounded (clock64 budget, ~1 s); on expiry the
 // kernel raises the error flag and continues without hanging.
@@ -21,18 +27,20 @@ namespace daw {
 namespace {
 
 constexpr int TR = 64;        // rows per tile
-constexpr int TC = 16;        // columns per tile
+constexpr int TC = 32;        // columns per tile
+constexpr int CPT = 4;        // columns per thread (8 warps x 4 = TC)
 constexpr int HR = 4;         // row halo (16-byte aligned TMA start)
 constexpr int kThreadsT = 256;
 constexpr unsigned kAll = 0xffffffffu;
 
 // stage layouts (bytes, 128-aligned sections)
-constexpr int kPVX = TR * (TC + 3) * 4;       // 4864  vx, columns c0-2..c0+TC
-constexpr int kPVZ = (TR + 2 * HR) * TC * 4;  // 4608  vz, rows r0-4..r0+TR+3
-constexpr int kPF = TR * TC * 4;              // 4096  px, pz, kappa
-constexpr int kPStage = kPVX + kPVZ + 3 * kPF;  // 21760
-constexpr int kVP = 5504;                     // p, 72 rows x 19 columns (5472, padded)
-constexpr int kVStage = kVP + 2 * kPF;        // 13696
+constexpr int kPVX = TR * (TC + 3) * 4;       // 8960  vx, columns c0-2..c0+TC
+constexpr int kPVZ = (TR + 2 * HR) * TC * 4;  // 9216  vz, rows r0-4..r0+TR+3
+constexpr int kPF = TR * TC * 4;              // 8192  px, pz, kappa
+constexpr int kPStage = kPVX + kPVZ + 3 * kPF;  // 42752
+constexpr int kVPb = (TR + 2 * HR) * (TC + 3) * 4;  // 10080 p, 72 rows x 35 columns
+constexpr int kVP = 10112;                    // (padded to 128)
+constexpr int kVStage = kVP + 2 * kPF;        // 26496
 constexpr int kGatherBytes = 8 * 444 * 4;     // 14208
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -154,6 +162,7 @@ __device__ __forceinline__ float inject_at(const InjMapDev& m, float v, int i1, 
   return v;
 }
 
+
 struct TileId {
   int shot, r0, c0;
 };
@@ -169,11 +178,29 @@ __device__ __forceinline__ TileId tile_id(const Grid& g, int t) {
   return id;
 }
 
+// Unscaled history values of a lane's two rows (FP16 bits converted to float
+// later, FP32 as is); both rows valid -> one aligned pair load.
+template <bool FP16>
+__device__ __forceinline__ float2 hist_raw(const void* base, int o, bool v0, bool v1) {
+  if (FP16) {
+    const __half* h = static_cast<const __half*>(base);
+    if (v0 && v1) return __half22float2(*reinterpret_cast<const __half2*>(h + o));
+    return make_float2(v0 ? __half2float(h[o]) : 0.f, v1 ? __half2float(h[o + 1]) : 0.f);
+  }
+  const float* f = static_cast<const float*>(base);
+  if (v0 && v1) return *reinterpret_cast<const float2*>(f + o);
+  return make_float2(v0 ? f[o] : 0.f, v1 ? f[o + 1] : 0.f);
+}
+
+__device__ __forceinline__ float2 ldg2(const float* p) {
+  return __ldg(reinterpret_cast<const float2*>(p));
+}
+
 // ---------------------------------------------------------------------------
 // Pressure kernel
 // ---------------------------------------------------------------------------
 template <int MODE, bool FP16>
-__global__ void __launch_bounds__(kThreadsT)
+__global__ void __launch_bounds__(kThreadsT, 2)
     k_tma_p(const Grid g, const ModelDev m, const FusedLaunch L, const int it, const int ntiles) {
   using H = Hist<FP16>;
   extern __shared__ __align__(128) unsigned char smem[];
@@ -200,8 +227,6 @@ __global__ void __launch_bounds__(kThreadsT)
   if (tid == 0 && t < ntiles) issue(t, 0);
   uint32_t phase0 = 0, phase1 = 0;
   int stage = 0;
-  int cur_shot = -1;
-  float lmax = 0.f;
   const int ld = g.ld, n1e = g.n1e, n2e = g.n2e, npml = g.npml;
   const int off = (MODE == FM_FWD) ? 2 : 3;
   const int hi1 = n1e - off, hi2 = n2e - off;
@@ -209,131 +234,152 @@ __global__ void __launch_bounds__(kThreadsT)
   const int n1h = L.n1h;
   const size_t nih = (size_t)n1h * g.n2;
   const float dtdx = g.dtdx, dt = g.dt, mdt = fmul(-1.0f, dt);
+  const int slo = (MODE == FM_STAGE_B_ES) ? 1 : 0;
+  const int shi1 = (MODE == FM_STAGE_B_ES) ? g.n1 - 1 : g.n1;
+  const int shi2 = (MODE == FM_STAGE_B_ES) ? g.n2 - 1 : g.n2;
+  // per-shot state (refreshed when the tile's shot changes; CTA-uniform)
+  int cur = -1;
+  ShotDevice sd;
+  bool live = false, flush = false, do_inj = false;
+  float inv_vx = 1.f, inv_vz = 1.f, sc_p = 1.f;
+  void* hvs = nullptr;
+  const void* hpr = nullptr;
+  float lmax = 0.f;
   for (; t < ntiles; t += gridDim.x) {
     const int tn = t + gridDim.x;
     if (tid == 0 && tn < ntiles) issue(tn, stage ^ 1);
     const TileId id = tile_id(g, t);
-    const ShotDevice sd = L.shots[id.shot];
-    if (MODE == FM_STAGE_A && id.shot != cur_shot) {
-      if (cur_shot >= 0) {
-        const ShotDevice& so = L.shots[cur_shot];
-        warp_amax_flush(lmax, so.amax + (size_t)(it - 1) * 3 * kAmaxSlots +
+    if (id.shot != cur) {
+      if (MODE == FM_STAGE_A && cur >= 0 && live && !flush)
+        warp_amax_flush(lmax, sd.amax + (size_t)(it - 1) * 3 * kAmaxSlots +
                                   ((blockIdx.x * 8 + warp) % kAmaxSlots));
-      }
-      cur_shot = id.shot;
+      cur = id.shot;
+      sd = L.shots[cur];
+      const int nt = sd.nt;
+      live = sd.active && (MODE == FM_STAGE_A ? it <= nt + 1 : it <= nt);
+      flush = (MODE == FM_STAGE_A) && it == nt + 1;
+      do_inj = (MODE == FM_STAGE_A) || (MODE == FM_FWD && sd.type_src == 0);
       lmax = 0.f;
+      const int ic = nt - it + 1;
+      if (live && MODE == FM_STAGE_A && it >= 2) {
+        hvs = step_ptr<FP16>(sd.hist, it - 2, nih);
+        if (FP16) {
+          const unsigned* a = sd.amax + (size_t)(it - 2) * 3 * kAmaxSlots;
+          inv_vx = pow2f(15 - amax_exponent(warp_amax_slots(a + kAmaxSlots)));
+          inv_vz = pow2f(15 - amax_exponent(warp_amax_slots(a + 2 * kAmaxSlots)));
+        }
+      }
+      if (live && (MODE == FM_STAGE_B || MODE == FM_STAGE_B_ES)) {
+        hpr = step_ptr<FP16>(sd.hist, ic - 1, nih);
+        if (FP16)
+          sc_p = pow2f(amax_exponent(warp_amax_slots(sd.amax + (size_t)(ic - 1) * 3 * kAmaxSlots)) - 15);
+      }
     }
-    const int nt = sd.nt;
-    const bool live = sd.active && (MODE == FM_STAGE_A ? it <= nt + 1 : it <= nt);
-    const bool flush = (MODE == FM_STAGE_A) && it == nt + 1;
-    const int ic = nt - it + 1;
     const int i1 = id.r0 + 2 * lane;
     const bool ok0 = i1 < n1e, ok1 = i1 + 1 < n1e;
     const bool u0 = ok0 && i1 >= 2 && i1 < hi1, u1 = ok1 && i1 + 1 >= 2 && i1 + 1 < hi1;
     const bool r0 = ok0 && i1 >= npml && i1 < npml + g.n1;
     const bool r1 = ok1 && i1 + 1 >= npml && i1 + 1 < npml + g.n1;
     const int h1 = i1 - npml + (npml & 1);
-    // stage-B history (HBM stream) issued before waiting on the tile
-    float sc_p = 1.f, inv_vx = 1.f, inv_vz = 1.f;
-    float2 hv[2] = {make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
-    const int slo = (MODE == FM_STAGE_B_ES) ? 1 : 0;
-    const int shi1 = (MODE == FM_STAGE_B_ES) ? g.n1 - 1 : g.n1;
-    const int shi2 = (MODE == FM_STAGE_B_ES) ? g.n2 - 1 : g.n2;
     const bool s0 = r0 && i1 - npml >= slo && i1 - npml < shi1;
     const bool s1 = r1 && i1 + 1 - npml >= slo && i1 + 1 - npml < shi1;
-    if (live && (MODE == FM_STAGE_B || MODE == FM_STAGE_B_ES)) {
-      if (FP16) sc_p = pow2f(amax_exponent(warp_amax_slots(sd.amax + (size_t)(ic - 1) * 3 * kAmaxSlots)) - 15);
-      const void* hp = step_ptr<FP16>(sd.hist, ic - 1, nih);
-#pragma unroll
-      for (int j = 0; j < 2; ++j) {
-        const int c = id.c0 + 2 * warp + j;
-        const int i2p = c - npml;
-        if (c < n2e && i2p >= slo && i2p < shi2 && (s0 || s1))
-          hv[j] = H::get2(hp, h1 + n1h * i2p, sc_p, s0, s1);
+    const int cb = id.c0 + CPT * warp;  // first column of this thread
+    // ---- global prefetch before waiting for the tile
+    float2 d1a = make_float2(0.f, 0.f), d1a1 = make_float2(0.f, 0.f);
+    float d2a[CPT], d2a1[CPT];
+    int clo[CPT], chi[CPT];
+    float2 hv[CPT];
+    if (live && !flush) {
+      if (ok1) {
+        d1a = ldg2(m.d1a + i1);
+        d1a1 = ldg2(m.d1a1 + i1);
+      } else if (ok0) {
+        d1a.x = __ldg(m.d1a + i1);
+        d1a1.x = __ldg(m.d1a1 + i1);
       }
     }
-    if (live && FP16 && MODE == FM_STAGE_A && it >= 2) {
-      const unsigned* a = sd.amax + (size_t)(it - 2) * 3 * kAmaxSlots;
-      inv_vx = pow2f(15 - amax_exponent(warp_amax_slots(a + kAmaxSlots)));
-      inv_vz = pow2f(15 - amax_exponent(warp_amax_slots(a + 2 * kAmaxSlots)));
+#pragma unroll
+    for (int j = 0; j < CPT; ++j) {
+      const int c = cb + j;
+      const bool cok = live && !flush && c < n2e;
+      d2a[j] = cok ? __ldg(m.d2a + c) : 0.f;
+      d2a1[j] = cok ? __ldg(m.d2a1 + c) : 0.f;
+      clo[j] = (cok && do_inj) ? __ldg(sd.inj.col_lo + c) : 0x7fffffff;
+      chi[j] = (cok && do_inj) ? __ldg(sd.inj.col_hi + c) : -1;
+      hv[j] = make_float2(0.f, 0.f);
+      if (MODE == FM_STAGE_B || MODE == FM_STAGE_B_ES) {
+        const int i2p = c - npml;
+        if (cok && i2p >= slo && i2p < shi2 && (s0 || s1))
+          hv[j] = hist_raw<FP16>(hpr, h1 + n1h * i2p, s0, s1);
+      }
     }
     bar_wait(&bar[stage], stage ? phase1 : phase0, L.err);
     if (stage) phase1 ^= 1; else phase0 ^= 1;
     const unsigned char* st = smem + stage * kPStage;
-    const float2* VX = reinterpret_cast<const float2*>(st);              // [TC+3][32]
-    const float* VZ = reinterpret_cast<const float*>(st + kPVX);         // [TC][72]
+    const float2* VX = reinterpret_cast<const float2*>(st);         // [TC+3][32]
+    const float* VZ = reinterpret_cast<const float*>(st + kPVX);    // [TC][72]
     const float2* PX = reinterpret_cast<const float2*>(st + kPVX + kPVZ);
     const float2* PZ = PX + TR * TC / 2;
     const float2* KA = PZ + TR * TC / 2;
-    if (live) {
-      void* hvs = (MODE == FM_STAGE_A && it >= 2) ? step_ptr<FP16>(sd.hist, it - 2, nih) : nullptr;
-      const bool do_inj = (MODE == FM_STAGE_A) || (MODE == FM_FWD && sd.type_src == 0);
-      const float2 d1a = ok1 ? __ldg(reinterpret_cast<const float2*>(m.d1a + i1))
-                             : make_float2(ok0 ? __ldg(m.d1a + i1) : 0.f, 0.f);
-      const float2 d1a1 = ok1 ? __ldg(reinterpret_cast<const float2*>(m.d1a1 + i1))
-                              : make_float2(ok0 ? __ldg(m.d1a1 + i1) : 0.f, 0.f);
+    if (live && ok0) {
+      float2 q[CPT + 3];  // vx at columns cb-2 .. cb+CPT
 #pragma unroll
-      for (int j = 0; j < 2; ++j) {
-        const int cc = 2 * warp + j;
+      for (int k = 0; k < CPT + 3; ++k) q[k] = VX[(CPT * warp + k) * 32 + lane];
+#pragma unroll
+      for (int j = 0; j < CPT; ++j) {
+        const int cc = CPT * warp + j;
         const int c = id.c0 + cc;
-        if (c >= n2e || !ok0) continue;
+        if (c >= n2e) continue;
         const int k = i1 + ld * c;
-        const float2 q0 = VX[(cc + 0) * 32 + lane], q1 = VX[(cc + 1) * 32 + lane];
-        const float2 q2 = VX[(cc + 2) * 32 + lane], q3 = VX[(cc + 3) * 32 + lane];
-        const float* vzc = VZ + cc * (TR + 2 * HR) + 2 * lane;  // row r0+2l-4
-        const float2 zm = *reinterpret_cast<const float2*>(vzc + 2);  // rows i1-2, i1-1
-        const float2 z = *reinterpret_cast<const float2*>(vzc + 4);   // rows i1, i1+1
-        const float zp2 = vzc[6];                                     // row i1+2
+        const float* vzc = VZ + cc * (TR + 2 * HR) + 2 * lane;  // row i1-4
+        const float2 zm = *reinterpret_cast<const float2*>(vzc + 2);
+        const float2 z = *reinterpret_cast<const float2*>(vzc + 4);
+        const float zp2 = vzc[6];
         const int i2p = c - npml;
         const bool cint = i2p >= 0 && i2p < g.n2;
         if (MODE == FM_STAGE_A && it >= 2 && cint && (r0 || r1)) {
           const int ho = h1 + n1h * i2p;
-          H::put2(hvs, (int)nih + ho, q2.x, q2.y, inv_vx, r0, r1);
+          H::put2(hvs, (int)nih + ho, q[j + 2].x, q[j + 2].y, inv_vx, r0, r1);
           H::put2(hvs, 2 * (int)nih + ho, z.x, z.y, inv_vz, r0, r1);
         }
         if (flush) continue;
         float2 px_ = PX[cc * 32 + lane], pz_ = PZ[cc * 32 + lane];
         const float2 kv = KA[cc * 32 + lane];
         if (c >= 2 && c < hi2) {
-          const float kw2f = __ldg(m.d2a1 + c), d2a = __ldg(m.d2a + c);
           const bool fwd = (MODE != FM_STAGE_A);
           if (u0) {
-            const float der2 = dminus(q0.x, q1.x, q2.x, q3.x);
+            const float der2 = dminus(q[j].x, q[j + 1].x, q[j + 2].x, q[j + 3].x);
             const float der1 = dminus(zm.x, zm.y, z.x, z.y);
             const float kd = fmul(dtdx, kv.x);
-            const float ax = fmul(d2a, px_.x), bx = fmul(fmul(kd, kw2f), der2);
+            const float ax = fmul(d2a[j], px_.x), bx = fmul(fmul(kd, d2a1[j]), der2);
             const float az = fmul(d1a.x, pz_.x), bz = fmul(fmul(kd, d1a1.x), der1);
             px_.x = fwd ? fadd(ax, bx) : fsub(ax, bx);
             pz_.x = fwd ? fadd(az, bz) : fsub(az, bz);
           }
           if (u1) {
-            const float der2 = dminus(q0.y, q1.y, q2.y, q3.y);
+            const float der2 = dminus(q[j].y, q[j + 1].y, q[j + 2].y, q[j + 3].y);
             const float der1 = dminus(zm.y, z.x, z.y, zp2);
             const float kd = fmul(dtdx, kv.y);
-            const float ax = fmul(d2a, px_.y), bx = fmul(fmul(kd, kw2f), der2);
+            const float ax = fmul(d2a[j], px_.y), bx = fmul(fmul(kd, d2a1[j]), der2);
             const float az = fmul(d1a.y, pz_.y), bz = fmul(fmul(kd, d1a1.y), der1);
             px_.y = fwd ? fadd(ax, bx) : fsub(ax, bx);
             pz_.y = fwd ? fadd(az, bz) : fsub(az, bz);
           }
         }
-        if (do_inj) {
-          const int clo = __ldg(sd.inj.col_lo + c);
-          const int chi = __ldg(sd.inj.col_hi + c);
-          if (i1 + 1 >= clo && i1 <= chi) {
-            const int base = __ldg(sd.inj.col_base + c);
-            const int sg = MODE == FM_FWD ? +1 : -1;
-            if (i1 >= clo && i1 <= chi)
-              px_.x = inject_at(sd.inj, px_.x, i1, clo, base, dt, kv.x, sd.amp + (it - 1),
-                                sd.amp_stride, sg);
-            if (ok1 && i1 + 1 >= clo && i1 + 1 <= chi)
-              px_.y = inject_at(sd.inj, px_.y, i1 + 1, clo, base, dt, kv.y, sd.amp + (it - 1),
-                                sd.amp_stride, sg);
-          }
+        if (i1 + 1 >= clo[j] && i1 <= chi[j]) {  // injection band (forward source / stage-A receivers)
+          const int base = __ldg(sd.inj.col_base + c);
+          const int sg = MODE == FM_FWD ? +1 : -1;
+          if (i1 >= clo[j])
+            px_.x = inject_at(sd.inj, px_.x, i1, clo[j], base, dt, kv.x, sd.amp + (it - 1),
+                              sd.amp_stride, sg);
+          if (ok1 && i1 + 1 <= chi[j])
+            px_.y = inject_at(sd.inj, px_.y, i1 + 1, clo[j], base, dt, kv.y, sd.amp + (it - 1),
+                              sd.amp_stride, sg);
         }
         if (MODE == FM_STAGE_B || MODE == FM_STAGE_B_ES) {
           if (i2p >= slo && i2p < shi2) {
-            if (s0) px_.x = fadd(px_.x, fmul(fmul(mdt, hv[j].x), kv.x));
-            if (s1) px_.y = fadd(px_.y, fmul(fmul(mdt, hv[j].y), kv.y));
+            if (s0) px_.x = fadd(px_.x, fmul(fmul(mdt, hv[j].x * sc_p), kv.x));
+            if (s1) px_.y = fadd(px_.y, fmul(fmul(mdt, hv[j].y * sc_p), kv.y));
           }
         }
         float2 pv;
@@ -364,21 +410,19 @@ __global__ void __launch_bounds__(kThreadsT)
     __syncthreads();  // stage buffer free for the copy issued next iteration
     stage ^= 1;
   }
-  if (MODE == FM_STAGE_A && cur_shot >= 0) {
-    const ShotDevice& so = L.shots[cur_shot];
-    warp_amax_flush(lmax, so.amax + (size_t)(it - 1) * 3 * kAmaxSlots +
+  if (MODE == FM_STAGE_A && cur >= 0 && live && !flush)
+    warp_amax_flush(lmax, sd.amax + (size_t)(it - 1) * 3 * kAmaxSlots +
                               ((blockIdx.x * 8 + warp) % kAmaxSlots));
-  }
 }
 
 // ---------------------------------------------------------------------------
-// Velocity kernel; gather tiles (8 stations each) come first.
+// Velocity kernel; gather work (8 stations per CTA pass) runs first, while
+// the first tile's copies are in flight.
 // ---------------------------------------------------------------------------
 template <int MODE, bool FP16>
-__global__ void __launch_bounds__(kThreadsT)
+__global__ void __launch_bounds__(kThreadsT, 2)
     k_tma_v(const Grid g, const ModelDev m, const FusedLaunch L, const int it, const int ntiles,
             const int ngb_per_shot) {
-  using H = Hist<FP16>;
   extern __shared__ __align__(128) unsigned char smem[];
   uint64_t* bar = reinterpret_cast<uint64_t*>(smem + 2 * kVStage);
   float* prod = reinterpret_cast<float*>(smem + 2 * kVStage + 128);
@@ -393,43 +437,40 @@ __global__ void __launch_bounds__(kThreadsT)
     const TileId id = tile_id(g, t);
     const TmaMaps* mp = L.maps + id.shot;
     unsigned char* st = smem + s * kVStage;
-    bar_expect(&bar[s], TR * (TC + 3) * 4 + HR * 2 * (TC + 3) * 4 + 2 * kPF);
+    bar_expect(&bar[s], kVPb + 2 * kPF);
     tma_2d(st, &mp->p72, id.r0 - HR, id.c0 - 1, &bar[s]);
     tma_2d(st + kVP, &mp->vx16, id.r0, id.c0, &bar[s]);
     tma_2d(st + kVP + kPF, &mp->vz16, id.r0, id.c0, &bar[s]);
   };
   int t = blockIdx.x;
   if (tid == 0 && t < ntiles) issue(t, 0);
-  // gathers while the first tile is in flight
   if (MODE != FM_STAGE_A) {
     const int ngb = ngb_per_shot * L.nshots;
     for (int gb = blockIdx.x; gb < ngb; gb += gridDim.x) {
       const int shot = gb / ngb_per_shot;
-      const ShotDevice& sd = L.shots[shot];
-      if (!sd.active || it > sd.nt || sd.type_rec != 0) continue;
+      const ShotDevice& so = L.shots[shot];
+      if (!so.active || it > so.nt || so.type_rec != 0) continue;
       const int s = (gb % ngb_per_shot) * 8 + warp;
-      if (s < sd.rec.n) {
-        if (sd.out) {
-          const float v = warp_gather_ordered(prod + warp * 444, sd.rec.ix1, sd.rec.ix2,
-                                              sd.rec.tile, s, sd.p, g.ld, 0, g.n1e, g.n2e);
-          const int row = sd.out_reverse ? sd.nt - it : it - 1;
-          if (lane == 0) sd.out[row + (size_t)sd.nt * s] = v;
+      if (s < so.rec.n) {
+        if (so.out) {
+          const float v = warp_gather_ordered(prod + warp * 444, so.rec.ix1, so.rec.ix2,
+                                              so.rec.tile, s, so.p, g.ld, 0, g.n1e, g.n2e);
+          const int row = so.out_reverse ? so.nt - it : it - 1;
+          if (lane == 0) so.out[row + (size_t)so.nt * s] = v;
         }
-      } else if (s - sd.rec.n < sd.datum.n && sd.red &&
+      } else if (s - so.rec.n < so.datum.n && so.red &&
                  (MODE == FM_FWD || MODE == FM_STAGE_B_ES)) {
-        const int d = s - sd.rec.n;
-        const float v = warp_gather_ordered(prod + warp * 444, sd.datum.ix1, sd.datum.ix2,
-                                            sd.datum.tile, d,
-                                            sd.p + g.npml + (size_t)g.ld * g.npml, g.ld,
+        const int d = s - so.rec.n;
+        const float v = warp_gather_ordered(prod + warp * 444, so.datum.ix1, so.datum.ix2,
+                                            so.datum.tile, d,
+                                            so.p + g.npml + (size_t)g.ld * g.npml, g.ld,
                                             g.npml, g.n1, g.n2);
-        if (lane == 0) sd.red[(it - 1) + (size_t)sd.nt * d] = v;
+        if (lane == 0) so.red[(it - 1) + (size_t)so.nt * d] = v;
       }
     }
   }
   uint32_t phase0 = 0, phase1 = 0;
   int stage = 0;
-  int cur_shot = -1;
-  float lmx = 0.f, lmz = 0.f;
   const int ld = g.ld, n1e = g.n1e, n2e = g.n2e, npml = g.npml;
   const int off = (MODE == FM_FWD) ? 2 : 3;
   const int hi1 = n1e - off, hi2 = n2e - off;
@@ -437,101 +478,123 @@ __global__ void __launch_bounds__(kThreadsT)
   const size_t nih = (size_t)n1h * g.n2;
   const float dt = g.dt, mdt = fmul(-1.0f, dt);
   const bool fs = g.ofs == 1;
+  int cur = -1;
+  ShotDevice sd;
+  bool live = false, do_inj = false;
+  float inv_p = 1.f, sc_vx = 1.f, sc_vz = 1.f;
+  void* hps = nullptr;
+  const void* hvr = nullptr;
+  float lmx = 0.f, lmz = 0.f;
   for (; t < ntiles; t += gridDim.x) {
     const int tn = t + gridDim.x;
     if (tid == 0 && tn < ntiles) issue(tn, stage ^ 1);
     const TileId id = tile_id(g, t);
-    const ShotDevice sd = L.shots[id.shot];
-    if (MODE == FM_STAGE_A && id.shot != cur_shot) {
-      if (cur_shot >= 0) {
-        unsigned* a = L.shots[cur_shot].amax + (size_t)(it - 1) * 3 * kAmaxSlots +
-                      ((blockIdx.x * 8 + warp) % kAmaxSlots);
+    if (id.shot != cur) {
+      if (MODE == FM_STAGE_A && cur >= 0 && live) {
+        unsigned* a = sd.amax + (size_t)(it - 1) * 3 * kAmaxSlots + ((blockIdx.x * 8 + warp) % kAmaxSlots);
         warp_amax_flush(lmx, a + kAmaxSlots);
         warp_amax_flush(lmz, a + 2 * kAmaxSlots);
       }
-      cur_shot = id.shot;
+      cur = id.shot;
+      sd = L.shots[cur];
+      live = sd.active && it <= sd.nt;
+      do_inj = (MODE == FM_FWD) && sd.type_src == 1;
       lmx = lmz = 0.f;
+      const int ic = sd.nt - it + 1;
+      if (live && MODE == FM_STAGE_A) {
+        hps = step_ptr<FP16>(sd.hist, it - 1, nih);
+        if (FP16)
+          inv_p = pow2f(15 - amax_exponent(warp_amax_slots(sd.amax + (size_t)(it - 1) * 3 * kAmaxSlots)));
+      }
+      if (live && (MODE == FM_STAGE_B || MODE == FM_STAGE_B_ES)) {
+        hvr = step_ptr<FP16>(sd.hist, ic - 1, nih);
+        if (FP16) {
+          const unsigned* a = sd.amax + (size_t)(ic - 1) * 3 * kAmaxSlots;
+          sc_vx = pow2f(amax_exponent(warp_amax_slots(a + kAmaxSlots)) - 15);
+          sc_vz = pow2f(amax_exponent(warp_amax_slots(a + 2 * kAmaxSlots)) - 15);
+        }
+      }
     }
-    const int nt = sd.nt;
-    const bool live = sd.active && it <= nt;
-    const int ic = nt - it + 1;
     const int i1 = id.r0 + 2 * lane;
     const bool ok0 = i1 < n1e, ok1 = i1 + 1 < n1e;
     const bool u0 = ok0 && i1 >= 2 && i1 < hi1, u1 = ok1 && i1 + 1 >= 2 && i1 + 1 < hi1;
     const bool r0 = ok0 && i1 >= npml && i1 < npml + g.n1;
     const bool r1 = ok1 && i1 + 1 >= npml && i1 + 1 < npml + g.n1;
     const int h1 = i1 - npml + (npml & 1);
-    float inv_p = 1.f;
-    float2 hx[2] = {make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
-    float2 hz[2] = {make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
-    if (live && (MODE == FM_STAGE_B || MODE == FM_STAGE_B_ES)) {
-      float sc_vx = 1.f, sc_vz = 1.f;
-      if (FP16) {
-        const unsigned* a = sd.amax + (size_t)(ic - 1) * 3 * kAmaxSlots;
-        sc_vx = pow2f(amax_exponent(warp_amax_slots(a + kAmaxSlots)) - 15);
-        sc_vz = pow2f(amax_exponent(warp_amax_slots(a + 2 * kAmaxSlots)) - 15);
+    const int cb = id.c0 + CPT * warp;
+    // ---- global prefetch before waiting for the tile
+    float2 d1b = make_float2(0.f, 0.f), bw1 = make_float2(0.f, 0.f);
+    if (live) {
+      if (ok1) {
+        d1b = ldg2(m.d1b + i1);
+        bw1 = ldg2(m.bw1 + i1);
+      } else if (ok0) {
+        d1b.x = __ldg(m.d1b + i1);
+        bw1.x = __ldg(m.bw1 + i1);
       }
-      const void* hp = step_ptr<FP16>(sd.hist, ic - 1, nih);
+    }
+    float d2b[CPT], bw2[CPT];
+    int clo[CPT], chi[CPT];
+    float2 hx[CPT], hz[CPT];
 #pragma unroll
-      for (int j = 0; j < 2; ++j) {
-        const int c = id.c0 + 2 * warp + j;
+    for (int j = 0; j < CPT; ++j) {
+      const int c = cb + j;
+      const bool cok = live && c < n2e;
+      d2b[j] = cok ? __ldg(m.d2b + c) : 0.f;
+      bw2[j] = cok ? __ldg(m.bw2 + c) : 0.f;
+      clo[j] = (cok && do_inj) ? __ldg(sd.inj.col_lo + c) : 0x7fffffff;
+      chi[j] = (cok && do_inj) ? __ldg(sd.inj.col_hi + c) : -1;
+      hx[j] = hz[j] = make_float2(0.f, 0.f);
+      if (MODE == FM_STAGE_B || MODE == FM_STAGE_B_ES) {
         const int i2p = c - npml;
-        if (c < n2e && i2p >= 0 && i2p < g.n2 && (r0 || r1)) {
+        if (cok && i2p >= 0 && i2p < g.n2 && (r0 || r1)) {
           const int ho = h1 + n1h * i2p;
-          hx[j] = H::get2(hp, (int)nih + ho, sc_vx, r0, r1);
-          hz[j] = H::get2(hp, 2 * (int)nih + ho, sc_vz, r0, r1);
+          hx[j] = hist_raw<FP16>(hvr, (int)nih + ho, r0, r1);
+          hz[j] = hist_raw<FP16>(hvr, 2 * (int)nih + ho, r0, r1);
         }
       }
     }
-    if (live && FP16 && MODE == FM_STAGE_A)
-      inv_p = pow2f(15 - amax_exponent(warp_amax_slots(sd.amax + (size_t)(it - 1) * 3 * kAmaxSlots)));
     bar_wait(&bar[stage], stage ? phase1 : phase0, L.err);
     if (stage) phase1 ^= 1; else phase0 ^= 1;
     const unsigned char* st = smem + stage * kVStage;
-    const float* P = reinterpret_cast<const float*>(st);  // [TC+3][72], row 0 = r0-4, col 0 = c0-1
+    const float* P = reinterpret_cast<const float*>(st);  // [TC+3][72]: row 0 = r0-4, col 0 = c0-1
+    const float2* P2 = reinterpret_cast<const float2*>(st);
     const float2* VX = reinterpret_cast<const float2*>(st + kVP);
     const float2* VZ = VX + TR * TC / 2;
-    if (live) {
-      void* hps = (MODE == FM_STAGE_A) ? step_ptr<FP16>(sd.hist, it - 1, nih) : nullptr;
-      const bool do_inj = (MODE == FM_FWD) && sd.type_src == 1;
-      const float2 d1b = ok1 ? __ldg(reinterpret_cast<const float2*>(m.d1b + i1))
-                             : make_float2(ok0 ? __ldg(m.d1b + i1) : 0.f, 0.f);
-      const float2 bw1 = ok1 ? __ldg(reinterpret_cast<const float2*>(m.bw1 + i1))
-                             : make_float2(ok0 ? __ldg(m.bw1 + i1) : 0.f, 0.f);
+    if (live && ok0) {
+      float2 a[CPT + 3];  // p rows (i1, i1+1) at columns cb-1 .. cb+CPT+1
+#pragma unroll
+      for (int k = 0; k < CPT + 3; ++k) a[k] = P2[(CPT * warp + k) * ((TR + 2 * HR) / 2) + 2 + lane];
       const bool dst_x = fs && i1 == npml - 1;
       const bool skip_y = fs && i1 + 1 == npml - 1;
       const bool src_x = fs && i1 == npml;
 #pragma unroll
-      for (int j = 0; j < 2; ++j) {
-        const int cc = 2 * warp + j;
+      for (int j = 0; j < CPT; ++j) {
+        const int cc = CPT * warp + j;
         const int c = id.c0 + cc;
-        if (c >= n2e || !ok0) continue;
+        if (c >= n2e) continue;
         const int k = i1 + ld * c;
-        const float* pcol = P + (cc + 1) * (TR + 2 * HR) + 2 * lane;  // own column, row r0+2l-4
-        const float pm1 = pcol[3];                                           // row i1-1
-        const float2 pc = *reinterpret_cast<const float2*>(pcol + 4);        // rows i1, i1+1
-        const float2 pp = *reinterpret_cast<const float2*>(pcol + 6);        // rows i1+2, i1+3
-        const float2 a0 = *reinterpret_cast<const float2*>(P + cc * (TR + 2 * HR) + 2 * lane + 4);
-        const float2 a2 = *reinterpret_cast<const float2*>(P + (cc + 2) * (TR + 2 * HR) + 2 * lane + 4);
-        const float2 a3 = *reinterpret_cast<const float2*>(P + (cc + 3) * (TR + 2 * HR) + 2 * lane + 4);
+        const float* pcol = P + (cc + 1) * (TR + 2 * HR) + 2 * lane;  // own column, row i1-4
+        const float pm1 = pcol[3];
+        const float2 pc = a[j + 1];
+        const float2 pp = *reinterpret_cast<const float2*>(pcol + 6);
         const int i2p = c - npml;
         const bool cint = i2p >= 0 && i2p < g.n2;
         float2 vx_ = VX[cc * 32 + lane], vz_ = VZ[cc * 32 + lane];
         if (c >= 2 && c < hi2) {
-          const float d2b = __ldg(m.d2b + c), bw2 = __ldg(m.bw2 + c);
           const bool fwd = (MODE != FM_STAGE_A);
           if (u0) {
-            const float der2 = dplus(a0.x, pc.x, a2.x, a3.x);
+            const float der2 = dplus(a[j].x, pc.x, a[j + 2].x, a[j + 3].x);
             const float der1 = dplus(pm1, pc.x, pc.y, pp.x);
-            const float ax = fmul(d2b, vx_.x), bx = fmul(bw2, der2);
+            const float ax = fmul(d2b[j], vx_.x), bx = fmul(bw2[j], der2);
             const float az = fmul(d1b.x, vz_.x), bz = fmul(bw1.x, der1);
             vx_.x = fwd ? fadd(ax, bx) : fsub(ax, bx);
             vz_.x = fwd ? fadd(az, bz) : fsub(az, bz);
           }
           if (u1) {
-            const float der2 = dplus(a0.y, pc.y, a2.y, a3.y);
+            const float der2 = dplus(a[j].y, pc.y, a[j + 2].y, a[j + 3].y);
             const float der1 = dplus(pc.x, pc.y, pp.x, pp.y);
-            const float ax = fmul(d2b, vx_.y), bx = fmul(bw2, der2);
+            const float ax = fmul(d2b[j], vx_.y), bx = fmul(bw2[j], der2);
             const float az = fmul(d1b.y, vz_.y), bz = fmul(bw1.y, der1);
             vx_.y = fwd ? fadd(ax, bx) : fsub(ax, bx);
             vz_.y = fwd ? fadd(az, bz) : fsub(az, bz);
@@ -539,26 +602,22 @@ __global__ void __launch_bounds__(kThreadsT)
         }
         if ((MODE == FM_STAGE_B || MODE == FM_STAGE_B_ES) && cint) {
           if (r0) {
-            vx_.x = fadd(vx_.x, fmul(fmul(mdt, hx[j].x), 1.0f));
-            vz_.x = fadd(vz_.x, fmul(fmul(mdt, hz[j].x), 1.0f));
+            vx_.x = fadd(vx_.x, fmul(fmul(mdt, hx[j].x * sc_vx), 1.0f));
+            vz_.x = fadd(vz_.x, fmul(fmul(mdt, hz[j].x * sc_vz), 1.0f));
           }
           if (r1) {
-            vx_.y = fadd(vx_.y, fmul(fmul(mdt, hx[j].y), 1.0f));
-            vz_.y = fadd(vz_.y, fmul(fmul(mdt, hz[j].y), 1.0f));
+            vx_.y = fadd(vx_.y, fmul(fmul(mdt, hx[j].y * sc_vx), 1.0f));
+            vz_.y = fadd(vz_.y, fmul(fmul(mdt, hz[j].y * sc_vz), 1.0f));
           }
         }
-        if (do_inj) {
-          const int clo = __ldg(sd.inj.col_lo + c);
-          const int chi = __ldg(sd.inj.col_hi + c);
-          if (i1 + 1 >= clo && i1 <= chi) {
-            const int base = __ldg(sd.inj.col_base + c);
-            if (i1 >= clo && i1 <= chi)
-              vz_.x = inject_at(sd.inj, vz_.x, i1, clo, base, dt, 1.0f, sd.amp + (it - 1),
-                                sd.amp_stride, +1);
-            if (ok1 && i1 + 1 >= clo && i1 + 1 <= chi)
-              vz_.y = inject_at(sd.inj, vz_.y, i1 + 1, clo, base, dt, 1.0f, sd.amp + (it - 1),
-                                sd.amp_stride, +1);
-          }
+        if (i1 + 1 >= clo[j] && i1 <= chi[j]) {  // vz source (type_src = 1)
+          const int base = __ldg(sd.inj.col_base + c);
+          if (i1 >= clo[j])
+            vz_.x = inject_at(sd.inj, vz_.x, i1, clo[j], base, dt, 1.0f, sd.amp + (it - 1),
+                              sd.amp_stride, +1);
+          if (ok1 && i1 + 1 <= chi[j])
+            vz_.y = inject_at(sd.inj, vz_.y, i1 + 1, clo[j], base, dt, 1.0f, sd.amp + (it - 1),
+                              sd.amp_stride, +1);
         }
         if (dst_x) vz_.x = vz_.y;
         *reinterpret_cast<float2*>(sd.vx + k) = vx_;
@@ -568,7 +627,7 @@ __global__ void __launch_bounds__(kThreadsT)
           *reinterpret_cast<float2*>(sd.vz + k) = vz_;
         if (src_x) sd.vz[k - 1] = vz_.x;
         if (MODE == FM_STAGE_A && cint && (r0 || r1)) {
-          H::put2(hps, h1 + n1h * i2p, pc.x, pc.y, inv_p, r0, r1);
+          Hist<FP16>::put2(hps, h1 + n1h * i2p, pc.x, pc.y, inv_p, r0, r1);
           if (r0) {
             lmx = fmaxf(lmx, fabsf(vx_.x));
             lmz = fmaxf(lmz, fabsf(vz_.x));
@@ -583,9 +642,8 @@ __global__ void __launch_bounds__(kThreadsT)
     __syncthreads();
     stage ^= 1;
   }
-  if (MODE == FM_STAGE_A && cur_shot >= 0) {
-    unsigned* a = L.shots[cur_shot].amax + (size_t)(it - 1) * 3 * kAmaxSlots +
-                  ((blockIdx.x * 8 + warp) % kAmaxSlots);
+  if (MODE == FM_STAGE_A && cur >= 0 && live) {
+    unsigned* a = sd.amax + (size_t)(it - 1) * 3 * kAmaxSlots + ((blockIdx.x * 8 + warp) % kAmaxSlots);
     warp_amax_flush(lmx, a + kAmaxSlots);
     warp_amax_flush(lmz, a + 2 * kAmaxSlots);
   }
