@@ -57,6 +57,12 @@ struct Grid {
   float h, dt, dtdx;
   __host__ __device__ size_t ext_elems() const { return (size_t)ld * n2e; }
   __host__ __device__ size_t int_elems() const { return (size_t)n1 * n2; }
+  // Fused-path history layout [step][field][i2p][hist_rows]: extended row i1
+  // is stored at row i1 - hist_base, hist_base = npml rounded down to a
+  // multiple of 8, so a lane's (even, odd) row pair is aligned and a tile's
+  // first row is a 16-byte-aligned tensor-copy coordinate.
+  __host__ __device__ int hist_base() const { return npml & ~7; }
+  __host__ __device__ int hist_rows() const { return ((npml - (npml & ~7)) + n1 + 7) / 8 * 8; }
 };
 
 struct ModelDev {
@@ -87,8 +93,10 @@ struct InjMapDev {
   // Column-band view for the fused kernels.
   int* col_lo = nullptr;   // n2e: first touched row (0-based) or INT_MAX
   int* col_hi = nullptr;   // n2e: last touched row or -1
-  int* col_base = nullptr; // n2e: index into rowptr of row col_lo
-  int* rowptr = nullptr;   // dense rows of every band, +1: entry offsets
+  int* col_base = nullptr; // n2e: dense-row index of row col_lo
+  int* rowptr = nullptr;   // per dense row: [begin, end) entry offsets
+  float2* ent = nullptr;   // per entry: (coefficient, station index as int bits)
+  int nsta = 0;            // stations of the map
 };
 
 // ---------------------------------------------------------------------------

@@ -362,6 +362,15 @@ InjMapDev make_map(daw_handle* h, Pool& pool, const std::string& name, const int
   upload(m.col_hi, chi.data(), g.n2e * sizeof(int), h->st);
   upload(m.col_base, cbase.data(), g.n2e * sizeof(int), h->st);
   upload(m.rowptr, rp.data(), rp.size() * sizeof(int), h->st);
+  std::vector<float2> ent(sta.size());
+  for (size_t i = 0; i < sta.size(); ++i) {
+    float sbits;
+    std::memcpy(&sbits, &sta[i], sizeof sbits);
+    ent[i] = make_float2(coef[i], sbits);
+  }
+  m.ent = pool.get_t<float2>(name + ".ent", std::max<size_t>(1, ent.size()));
+  upload(m.ent, ent.data(), ent.size() * sizeof(float2), h->st);
+  m.nsta = n;
   sync(h);
   return m;
 }
@@ -371,9 +380,7 @@ InjMapDev make_map(daw_handle* h, Pool& pool, const std::string& name, const int
 // ---------------------------------------------------------------------------
 int hist_ld(const daw_handle* h) {
   // interior rows per column, padded to 8 elements (16 B of FP16)
-  // interior rows + 1 (the fused layout shifts rows by npml & 1 so a lane's
-  // row pair is aligned), padded to 8 elements (16 B of FP16)
-  return (h->g.n1 + 1 + 7) / 8 * 8;
+  return h->g.hist_rows();
 }
 size_t hist_bytes_per_step(const daw_handle* h, bool fp16) {
   return (size_t)3 * hist_ld(h) * h->g.n2 * (fp16 ? 2 : 4);
@@ -566,7 +573,8 @@ void fill_shot_devices(daw_handle* h, Batch& b, int mode) {
     std::vector<TmaMaps> maps(b.shots.size());
     for (size_t i = 0; i < b.shots.size(); ++i) {
       const ShotCtx& c = *b.shots[i];
-      if (!tma_encode_maps(h->g, c.vx, c.vz, c.px, c.pz, c.p, h->md.kap, &maps[i]))
+      if (!tma_encode_maps(h->g, c.vx, c.vz, c.px, c.pz, c.p, h->md.kap, c.hist,
+                           h->opt.history_fp16, hist_ld(h), c.nt, &maps[i]))
         throw DawError{DAW_ERR_CUDA, "cuTensorMapEncodeTiled failed"};
     }
     b.d_maps = static_cast<TmaMaps*>(
@@ -716,7 +724,7 @@ void batch_operator(daw_handle* h, Batch& b, bool esource) {
     if (!c->active) continue;
     if (esource && c->d_cost)
       history_cost(c->hist, h->opt.history_fp16, c->amax, c->nt, h->g.n1, h->g.n2, hist_ld(h),
-                   h->g.npml & 1, (size_t)hist_ld(h) * h->g.n2, c->d_cost, h->st);
+                   h->g.npml - h->g.hist_base(), (size_t)hist_ld(h) * h->g.n2, c->d_cost, h->st);
     zero_state(h, *c);
     CK(cudaMemsetAsync(c->op_out, 0, (size_t)c->nt * c->nr * sizeof(float), h->st));
     if (esource && h->ndatum)

@@ -47,7 +47,7 @@ struct ShotDevice {
 // 2-D tensor maps of one shot's fields for the TMA kernels (box sizes in
 // stencil_tma.cu): vx/vz/px/pz/p with their stencil halos, and kappa.
 struct alignas(64) TmaMaps {
-  CUtensorMap vx19, vz72, px, pz, p72, vx16, vz16, kap;
+  CUtensorMap vx19, vz72, px, pz, p72, vx16, vz16, kap, hist;
 };
 
 struct FusedLaunch {
@@ -70,7 +70,8 @@ void tma_p_step(const Grid& g, const ModelDev& m, const FusedLaunch& L, int mode
 void tma_v_step(const Grid& g, const ModelDev& m, const FusedLaunch& L, int mode, int it,
                 cudaStream_t st);
 bool tma_encode_maps(const Grid& g, const float* vx, const float* vz, const float* px,
-                     const float* pz, const float* p, const float* kap, TmaMaps* out);
+                     const float* pz, const float* p, const float* kap, const void* hist,
+                     int hist_fp16, int n1h, int nsteps, TmaMaps* out);
 
 // Stage-A flush at it = nt+1 is folded into fused_p_step (it may exceed a
 // shot's nt by one in stage A).

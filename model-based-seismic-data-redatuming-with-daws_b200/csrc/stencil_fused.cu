@@ -18,9 +18,9 @@
 // field reduces max|x| over the interior; the next kernel, which reads the
 // field anyway for its stencil, encodes and stores it -- no extra pass.
 //
-// History layout: [step][field][i2p][n1h] with interior row i1p stored at
-// i1p + (npml & 1), so the two rows of a lane (even extended row i1) land on
-// an aligned pair.
+// History layout: [step][field][i2p][n1h] with extended row i1 stored at row
+// i1 - Grid::hist_base(), so the two rows of a lane (even i1) land on an
+// aligned pair.
 #include "fused.cuh"
 
 namespace daw {
@@ -168,7 +168,7 @@ __global__ void __launch_bounds__(kThreads)
   const bool u0 = ok0 && i1 >= 2 && i1 < hi1, u1 = ok1 && i1 + 1 >= 2 && i1 + 1 < hi1;
   const bool r0 = ok0 && i1 >= npml && i1 < npml + g.n1;
   const bool r1 = ok1 && i1 + 1 >= npml && i1 + 1 < npml + g.n1;
-  const int h1 = i1 - npml + (npml & 1);  // history row of i1 (even)
+  const int h1 = i1 - g.hist_base();  // history row of i1 (even)
   const int ic = nt - it + 1;
 
   float inv_vx = 1.f, inv_vz = 1.f, sc_p = 1.f;
@@ -373,7 +373,7 @@ __global__ void __launch_bounds__(kThreads)
   const bool u0 = ok0 && i1 >= 2 && i1 < hi1, u1 = ok1 && i1 + 1 >= 2 && i1 + 1 < hi1;
   const bool r0 = ok0 && i1 >= npml && i1 < npml + g.n1;
   const bool r1 = ok1 && i1 + 1 >= npml && i1 + 1 < npml + g.n1;
-  const int h1 = i1 - npml + (npml & 1);
+  const int h1 = i1 - g.hist_base();
   const int ic = nt - it + 1;
   float inv_p = 1.f, sc_vx = 1.f, sc_vz = 1.f;
   if (FP16) {

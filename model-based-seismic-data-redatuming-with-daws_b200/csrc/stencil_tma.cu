@@ -42,6 +42,20 @@ constexpr int kVPb = (TR + 2 * HR) * (TC + 3) * 4;  // 10080 p, 72 rows x 35 col
 constexpr int kVP = 10112;                    // (padded to 128)
 constexpr int kVStage = kVP + 2 * kPF;        // 26496
 constexpr int kGatherBytes = 8 * 444 * 4;     // 14208
+constexpr int kAmpMax = 2048;                 // stations whose amplitudes are staged in smem
+constexpr int kAmpBytes = kAmpMax * 4;
+
+// Stage sizes by mode/precision: stage B adds the history box(es) of the
+// time-reversed step (64 x 32 elements per field).
+__host__ __device__ constexpr int hist_box(bool fp16) { return TR * TC * (fp16 ? 2 : 4); }
+__host__ __device__ constexpr int p_stage(int mode, bool fp16) {
+  return kPStage + ((mode == FM_STAGE_B || mode == FM_STAGE_B_ES) ? hist_box(fp16) : 0);
+}
+__host__ __device__ constexpr int v_stage(int mode, bool fp16) {
+  return kVStage + ((mode == FM_STAGE_B || mode == FM_STAGE_B_ES) ? 2 * hist_box(fp16) : 0);
+}
+constexpr size_t p_smem(int mode, bool fp16) { return 2 * p_stage(mode, fp16) + 16 + kAmpBytes; }
+constexpr size_t v_smem(int mode, bool fp16) { return 2 * v_stage(mode, fp16) + 128 + kGatherBytes; }
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return (uint32_t)__cvta_generic_to_shared(p);
@@ -83,6 +97,14 @@ __device__ __forceinline__ void tma_2d(void* dst, const CUtensorMap* map, int x,
       "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes"
       " [%0], [%1, {%2, %3}], [%4];" ::"r"(smem_u32(dst)),
       "l"(map), "r"(x), "r"(y), "r"(smem_u32(b))
+      : "memory");
+}
+__device__ __forceinline__ void tma_3d(void* dst, const CUtensorMap* map, int x, int y, int z,
+                                       uint64_t* b) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(smem_u32(dst)),
+      "l"(map), "r"(x), "r"(y), "r"(z), "r"(smem_u32(b))
       : "memory");
 }
 
@@ -149,14 +171,31 @@ __device__ __forceinline__ void* step_ptr(void* hist, int step0, size_t nih) {
   return static_cast<char*>(hist) + (size_t)step0 * 3 * nih * (FP16 ? 2 : 4);
 }
 
-__device__ __forceinline__ float inject_at(const InjMapDev& m, float v, int i1, int clo, int base,
-                                           float dt, float w, const float* amp, int amp_stride,
-                                           int sign) {
-  const int r = base + (i1 - clo);
+// Injection at row i1 of a column band: the (coefficient, station) entries
+// of the point in station order, amplitudes of this step staged in `amp`
+// (shared memory).
+__device__ __forceinline__ float inject_at(const InjMapDev& m, float v, int r, float dt, float w,
+                                           const float* amp, int sign) {
+  const int e0 = __ldg(m.rowptr + 2 * r), e1 = __ldg(m.rowptr + 2 * r + 1);
+#pragma unroll 4
+  for (int e = e0; e < e1; ++e) {
+    const float2 q = __ldg(m.ent + e);
+    const float term = fmul(fmul(fmul(q.x, dt), amp[__float_as_int(q.y)]), w);
+    v = sign > 0 ? fadd(v, term) : fsub(v, term);
+  }
+  return v;
+}
+
+// Same with the amplitudes read from global memory (more than kAmpMax
+// stations, or the vz source of type_src = 1).
+__device__ __forceinline__ float inject_at_global(const InjMapDev& m, float v, int r, float dt,
+                                                  float w, const float* amp, int amp_stride,
+                                                  int sign) {
   const int e0 = __ldg(m.rowptr + 2 * r), e1 = __ldg(m.rowptr + 2 * r + 1);
   for (int e = e0; e < e1; ++e) {
-    const float a = __ldg(amp + (size_t)__ldg(m.sta + e) * amp_stride);
-    const float term = fmul(fmul(fmul(__ldg(m.coef + e), dt), a), w);
+    const float2 q = __ldg(m.ent + e);
+    const float a = __ldg(amp + (size_t)__float_as_int(q.y) * amp_stride);
+    const float term = fmul(fmul(fmul(q.x, dt), a), w);
     v = sign > 0 ? fadd(v, term) : fsub(v, term);
   }
   return v;
@@ -178,22 +217,24 @@ __device__ __forceinline__ TileId tile_id(const Grid& g, int t) {
   return id;
 }
 
-// Unscaled history values of a lane's two rows (FP16 bits converted to float
-// later, FP32 as is); both rows valid -> one aligned pair load.
-template <bool FP16>
-__device__ __forceinline__ float2 hist_raw(const void* base, int o, bool v0, bool v1) {
-  if (FP16) {
-    const __half* h = static_cast<const __half*>(base);
-    if (v0 && v1) return __half22float2(*reinterpret_cast<const __half2*>(h + o));
-    return make_float2(v0 ? __half2float(h[o]) : 0.f, v1 ? __half2float(h[o + 1]) : 0.f);
-  }
-  const float* f = static_cast<const float*>(base);
-  if (v0 && v1) return *reinterpret_cast<const float2*>(f + o);
-  return make_float2(v0 ? f[o] : 0.f, v1 ? f[o + 1] : 0.f);
-}
-
 __device__ __forceinline__ float2 ldg2(const float* p) {
   return __ldg(reinterpret_cast<const float2*>(p));
+}
+
+// Two rows (2*lane, 2*lane+1) of column cc of a history box in shared memory.
+template <bool FP16>
+__device__ __forceinline__ float2 hist_box_read(const unsigned char* box, int cc, int lane) {
+  if (FP16)
+    return __half22float2(reinterpret_cast<const __half2*>(box)[cc * (TR / 2) + lane]);
+  return reinterpret_cast<const float2*>(box)[cc * (TR / 2) + lane];
+}
+
+// Stage the step's station amplitudes amp[(it-1) + s*stride] in shared memory
+// (CTA-wide; called at a shot change, which is CTA-uniform).
+__device__ __forceinline__ void stage_amp(float* amp_s, const float* amp, int stride, int nsta) {
+  const int n = min(nsta, kAmpMax);
+  for (int s = threadIdx.x; s < n; s += blockDim.x) amp_s[s] = __ldg(amp + (size_t)s * stride);
+  __syncthreads();
 }
 
 // ---------------------------------------------------------------------------
@@ -203,8 +244,11 @@ template <int MODE, bool FP16>
 __global__ void __launch_bounds__(kThreadsT, 2)
     k_tma_p(const Grid g, const ModelDev m, const FusedLaunch L, const int it, const int ntiles) {
   using H = Hist<FP16>;
+  constexpr bool kB = (MODE == FM_STAGE_B || MODE == FM_STAGE_B_ES);
+  constexpr int kStage = p_stage(MODE, FP16);
   extern __shared__ __align__(128) unsigned char smem[];
-  uint64_t* bar = reinterpret_cast<uint64_t*>(smem + 2 * kPStage);
+  uint64_t* bar = reinterpret_cast<uint64_t*>(smem + 2 * kStage);
+  float* amp_s = reinterpret_cast<float*>(smem + 2 * kStage + 16);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   if (tid == 0) {
     bar_init(&bar[0]);
@@ -212,16 +256,21 @@ __global__ void __launch_bounds__(kThreadsT, 2)
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   }
   __syncthreads();
+  const int hbase = g.hist_base();
   auto issue = [&](int t, int s) {
     const TileId id = tile_id(g, t);
     const TmaMaps* mp = L.maps + id.shot;
-    unsigned char* st = smem + s * kPStage;
-    bar_expect(&bar[s], kPStage);
+    unsigned char* st = smem + s * kStage;
+    bar_expect(&bar[s], kStage);  // kPStage (+ history box) = bytes copied
     tma_2d(st, &mp->vx19, id.r0, id.c0 - 2, &bar[s]);
     tma_2d(st + kPVX, &mp->vz72, id.r0 - HR, id.c0, &bar[s]);
     tma_2d(st + kPVX + kPVZ, &mp->px, id.r0, id.c0, &bar[s]);
     tma_2d(st + kPVX + kPVZ + kPF, &mp->pz, id.r0, id.c0, &bar[s]);
     tma_2d(st + kPVX + kPVZ + 2 * kPF, &mp->kap, id.r0, id.c0, &bar[s]);
+    if (kB) {  // pressure history of the time-reversed step
+      const int ic = L.shots[id.shot].nt - it + 1;
+      tma_3d(st + kPStage, &mp->hist, id.r0 - hbase, id.c0 - g.npml, (ic - 1) * 3, &bar[s]);
+    }
   };
   int t = blockIdx.x;
   if (tid == 0 && t < ntiles) issue(t, 0);
@@ -237,19 +286,17 @@ __global__ void __launch_bounds__(kThreadsT, 2)
   const int slo = (MODE == FM_STAGE_B_ES) ? 1 : 0;
   const int shi1 = (MODE == FM_STAGE_B_ES) ? g.n1 - 1 : g.n1;
   const int shi2 = (MODE == FM_STAGE_B_ES) ? g.n2 - 1 : g.n2;
-  // per-shot state (refreshed when the tile's shot changes; CTA-uniform)
   int cur = -1;
   ShotDevice sd;
-  bool live = false, flush = false, do_inj = false;
+  bool live = false, flush = false, do_inj = false, amp_smem = false;
   float inv_vx = 1.f, inv_vz = 1.f, sc_p = 1.f;
   void* hvs = nullptr;
-  const void* hpr = nullptr;
   float lmax = 0.f;
   for (; t < ntiles; t += gridDim.x) {
     const int tn = t + gridDim.x;
     if (tid == 0 && tn < ntiles) issue(tn, stage ^ 1);
     const TileId id = tile_id(g, t);
-    if (id.shot != cur) {
+    if (id.shot != cur) {  // CTA-uniform
       if (MODE == FM_STAGE_A && cur >= 0 && live && !flush)
         warp_amax_flush(lmax, sd.amax + (size_t)(it - 1) * 3 * kAmaxSlots +
                                   ((blockIdx.x * 8 + warp) % kAmaxSlots));
@@ -258,9 +305,8 @@ __global__ void __launch_bounds__(kThreadsT, 2)
       const int nt = sd.nt;
       live = sd.active && (MODE == FM_STAGE_A ? it <= nt + 1 : it <= nt);
       flush = (MODE == FM_STAGE_A) && it == nt + 1;
-      do_inj = (MODE == FM_STAGE_A) || (MODE == FM_FWD && sd.type_src == 0);
+      do_inj = live && !flush && ((MODE == FM_STAGE_A) || (MODE == FM_FWD && sd.type_src == 0));
       lmax = 0.f;
-      const int ic = nt - it + 1;
       if (live && MODE == FM_STAGE_A && it >= 2) {
         hvs = step_ptr<FP16>(sd.hist, it - 2, nih);
         if (FP16) {
@@ -269,26 +315,24 @@ __global__ void __launch_bounds__(kThreadsT, 2)
           inv_vz = pow2f(15 - amax_exponent(warp_amax_slots(a + 2 * kAmaxSlots)));
         }
       }
-      if (live && (MODE == FM_STAGE_B || MODE == FM_STAGE_B_ES)) {
-        hpr = step_ptr<FP16>(sd.hist, ic - 1, nih);
-        if (FP16)
-          sc_p = pow2f(amax_exponent(warp_amax_slots(sd.amax + (size_t)(ic - 1) * 3 * kAmaxSlots)) - 15);
-      }
+      if (live && kB && FP16)
+        sc_p = pow2f(amax_exponent(warp_amax_slots(sd.amax + (size_t)(nt - it) * 3 * kAmaxSlots)) - 15);
+      amp_smem = sd.inj.nsta <= kAmpMax;
+      if (do_inj && amp_smem) stage_amp(amp_s, sd.amp + (it - 1), sd.amp_stride, sd.inj.nsta);
     }
     const int i1 = id.r0 + 2 * lane;
     const bool ok0 = i1 < n1e, ok1 = i1 + 1 < n1e;
     const bool u0 = ok0 && i1 >= 2 && i1 < hi1, u1 = ok1 && i1 + 1 >= 2 && i1 + 1 < hi1;
     const bool r0 = ok0 && i1 >= npml && i1 < npml + g.n1;
     const bool r1 = ok1 && i1 + 1 >= npml && i1 + 1 < npml + g.n1;
-    const int h1 = i1 - npml + (npml & 1);
+    const int h1 = i1 - hbase;
     const bool s0 = r0 && i1 - npml >= slo && i1 - npml < shi1;
     const bool s1 = r1 && i1 + 1 - npml >= slo && i1 + 1 - npml < shi1;
-    const int cb = id.c0 + CPT * warp;  // first column of this thread
+    const int cb = id.c0 + CPT * warp;
     // ---- global prefetch before waiting for the tile
     float2 d1a = make_float2(0.f, 0.f), d1a1 = make_float2(0.f, 0.f);
     float d2a[CPT], d2a1[CPT];
     int clo[CPT], chi[CPT];
-    float2 hv[CPT];
     if (live && !flush) {
       if (ok1) {
         d1a = ldg2(m.d1a + i1);
@@ -306,16 +350,10 @@ __global__ void __launch_bounds__(kThreadsT, 2)
       d2a1[j] = cok ? __ldg(m.d2a1 + c) : 0.f;
       clo[j] = (cok && do_inj) ? __ldg(sd.inj.col_lo + c) : 0x7fffffff;
       chi[j] = (cok && do_inj) ? __ldg(sd.inj.col_hi + c) : -1;
-      hv[j] = make_float2(0.f, 0.f);
-      if (MODE == FM_STAGE_B || MODE == FM_STAGE_B_ES) {
-        const int i2p = c - npml;
-        if (cok && i2p >= slo && i2p < shi2 && (s0 || s1))
-          hv[j] = hist_raw<FP16>(hpr, h1 + n1h * i2p, s0, s1);
-      }
     }
     bar_wait(&bar[stage], stage ? phase1 : phase0, L.err);
     if (stage) phase1 ^= 1; else phase0 ^= 1;
-    const unsigned char* st = smem + stage * kPStage;
+    const unsigned char* st = smem + stage * kStage;
     const float2* VX = reinterpret_cast<const float2*>(st);         // [TC+3][32]
     const float* VZ = reinterpret_cast<const float*>(st + kPVX);    // [TC][72]
     const float2* PX = reinterpret_cast<const float2*>(st + kPVX + kPVZ);
@@ -366,21 +404,26 @@ __global__ void __launch_bounds__(kThreadsT, 2)
             pz_.y = fwd ? fadd(az, bz) : fsub(az, bz);
           }
         }
-        if (i1 + 1 >= clo[j] && i1 <= chi[j]) {  // injection band (forward source / stage-A receivers)
-          const int base = __ldg(sd.inj.col_base + c);
+        if (i1 + 1 >= clo[j] && i1 <= chi[j]) {  // forward source / stage-A receivers
+          const int base = __ldg(sd.inj.col_base + c) - clo[j];
           const int sg = MODE == FM_FWD ? +1 : -1;
-          if (i1 >= clo[j])
-            px_.x = inject_at(sd.inj, px_.x, i1, clo[j], base, dt, kv.x, sd.amp + (it - 1),
-                              sd.amp_stride, sg);
-          if (ok1 && i1 + 1 <= chi[j])
-            px_.y = inject_at(sd.inj, px_.y, i1 + 1, clo[j], base, dt, kv.y, sd.amp + (it - 1),
-                              sd.amp_stride, sg);
-        }
-        if (MODE == FM_STAGE_B || MODE == FM_STAGE_B_ES) {
-          if (i2p >= slo && i2p < shi2) {
-            if (s0) px_.x = fadd(px_.x, fmul(fmul(mdt, hv[j].x * sc_p), kv.x));
-            if (s1) px_.y = fadd(px_.y, fmul(fmul(mdt, hv[j].y * sc_p), kv.y));
+          if (amp_smem) {
+            if (i1 >= clo[j]) px_.x = inject_at(sd.inj, px_.x, base + i1, dt, kv.x, amp_s, sg);
+            if (ok1 && i1 + 1 <= chi[j])
+              px_.y = inject_at(sd.inj, px_.y, base + i1 + 1, dt, kv.y, amp_s, sg);
+          } else {
+            if (i1 >= clo[j])
+              px_.x = inject_at_global(sd.inj, px_.x, base + i1, dt, kv.x, sd.amp + (it - 1),
+                                       sd.amp_stride, sg);
+            if (ok1 && i1 + 1 <= chi[j])
+              px_.y = inject_at_global(sd.inj, px_.y, base + i1 + 1, dt, kv.y, sd.amp + (it - 1),
+                                       sd.amp_stride, sg);
           }
+        }
+        if (kB && i2p >= slo && i2p < shi2 && (s0 || s1)) {
+          const float2 hv = hist_box_read<FP16>(st + kPStage, cc, lane);
+          if (s0) px_.x = fadd(px_.x, fmul(fmul(mdt, hv.x * sc_p), kv.x));
+          if (s1) px_.y = fadd(px_.y, fmul(fmul(mdt, hv.y * sc_p), kv.y));
         }
         float2 pv;
         pv.x = i1 < fsrows ? 0.f : fadd(px_.x, pz_.x);
@@ -407,7 +450,7 @@ __global__ void __launch_bounds__(kThreadsT, 2)
         }
       }
     }
-    __syncthreads();  // stage buffer free for the copy issued next iteration
+    __syncthreads();  // stage buffer (and staged amplitudes) free for reuse
     stage ^= 1;
   }
   if (MODE == FM_STAGE_A && cur >= 0 && live && !flush)
@@ -416,16 +459,18 @@ __global__ void __launch_bounds__(kThreadsT, 2)
 }
 
 // ---------------------------------------------------------------------------
-// Velocity kernel; gather work (8 stations per CTA pass) runs first, while
-// the first tile's copies are in flight.
+// Velocity kernel.  The receiver / datum gathers (8 stations per unit) run
+// after the stencil tiles, on the CTAs that drew one tile fewer.
 // ---------------------------------------------------------------------------
 template <int MODE, bool FP16>
 __global__ void __launch_bounds__(kThreadsT, 2)
     k_tma_v(const Grid g, const ModelDev m, const FusedLaunch L, const int it, const int ntiles,
             const int ngb_per_shot) {
+  constexpr bool kB = (MODE == FM_STAGE_B || MODE == FM_STAGE_B_ES);
+  constexpr int kStage = v_stage(MODE, FP16);
   extern __shared__ __align__(128) unsigned char smem[];
-  uint64_t* bar = reinterpret_cast<uint64_t*>(smem + 2 * kVStage);
-  float* prod = reinterpret_cast<float*>(smem + 2 * kVStage + 128);
+  uint64_t* bar = reinterpret_cast<uint64_t*>(smem + 2 * kStage);
+  float* prod = reinterpret_cast<float*>(smem + 2 * kStage + 128);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   if (tid == 0) {
     bar_init(&bar[0]);
@@ -433,42 +478,24 @@ __global__ void __launch_bounds__(kThreadsT, 2)
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   }
   __syncthreads();
+  const int hbase = g.hist_base();
   auto issue = [&](int t, int s) {
     const TileId id = tile_id(g, t);
     const TmaMaps* mp = L.maps + id.shot;
-    unsigned char* st = smem + s * kVStage;
-    bar_expect(&bar[s], kVPb + 2 * kPF);
+    unsigned char* st = smem + s * kStage;
+    bar_expect(&bar[s], kVPb + 2 * kPF + (kB ? 2 * hist_box(FP16) : 0));  // bytes copied
     tma_2d(st, &mp->p72, id.r0 - HR, id.c0 - 1, &bar[s]);
     tma_2d(st + kVP, &mp->vx16, id.r0, id.c0, &bar[s]);
     tma_2d(st + kVP + kPF, &mp->vz16, id.r0, id.c0, &bar[s]);
+    if (kB) {  // velocity histories of the time-reversed step
+      const int ic = L.shots[id.shot].nt - it + 1;
+      tma_3d(st + kVStage, &mp->hist, id.r0 - hbase, id.c0 - g.npml, (ic - 1) * 3 + 1, &bar[s]);
+      tma_3d(st + kVStage + hist_box(FP16), &mp->hist, id.r0 - hbase, id.c0 - g.npml,
+             (ic - 1) * 3 + 2, &bar[s]);
+    }
   };
   int t = blockIdx.x;
   if (tid == 0 && t < ntiles) issue(t, 0);
-  if (MODE != FM_STAGE_A) {
-    const int ngb = ngb_per_shot * L.nshots;
-    for (int gb = blockIdx.x; gb < ngb; gb += gridDim.x) {
-      const int shot = gb / ngb_per_shot;
-      const ShotDevice& so = L.shots[shot];
-      if (!so.active || it > so.nt || so.type_rec != 0) continue;
-      const int s = (gb % ngb_per_shot) * 8 + warp;
-      if (s < so.rec.n) {
-        if (so.out) {
-          const float v = warp_gather_ordered(prod + warp * 444, so.rec.ix1, so.rec.ix2,
-                                              so.rec.tile, s, so.p, g.ld, 0, g.n1e, g.n2e);
-          const int row = so.out_reverse ? so.nt - it : it - 1;
-          if (lane == 0) so.out[row + (size_t)so.nt * s] = v;
-        }
-      } else if (s - so.rec.n < so.datum.n && so.red &&
-                 (MODE == FM_FWD || MODE == FM_STAGE_B_ES)) {
-        const int d = s - so.rec.n;
-        const float v = warp_gather_ordered(prod + warp * 444, so.datum.ix1, so.datum.ix2,
-                                            so.datum.tile, d,
-                                            so.p + g.npml + (size_t)g.ld * g.npml, g.ld,
-                                            g.npml, g.n1, g.n2);
-        if (lane == 0) so.red[(it - 1) + (size_t)so.nt * d] = v;
-      }
-    }
-  }
   uint32_t phase0 = 0, phase1 = 0;
   int stage = 0;
   const int ld = g.ld, n1e = g.n1e, n2e = g.n2e, npml = g.npml;
@@ -483,7 +510,6 @@ __global__ void __launch_bounds__(kThreadsT, 2)
   bool live = false, do_inj = false;
   float inv_p = 1.f, sc_vx = 1.f, sc_vz = 1.f;
   void* hps = nullptr;
-  const void* hvr = nullptr;
   float lmx = 0.f, lmz = 0.f;
   for (; t < ntiles; t += gridDim.x) {
     const int tn = t + gridDim.x;
@@ -498,21 +524,17 @@ __global__ void __launch_bounds__(kThreadsT, 2)
       cur = id.shot;
       sd = L.shots[cur];
       live = sd.active && it <= sd.nt;
-      do_inj = (MODE == FM_FWD) && sd.type_src == 1;
+      do_inj = live && (MODE == FM_FWD) && sd.type_src == 1;
       lmx = lmz = 0.f;
-      const int ic = sd.nt - it + 1;
       if (live && MODE == FM_STAGE_A) {
         hps = step_ptr<FP16>(sd.hist, it - 1, nih);
         if (FP16)
           inv_p = pow2f(15 - amax_exponent(warp_amax_slots(sd.amax + (size_t)(it - 1) * 3 * kAmaxSlots)));
       }
-      if (live && (MODE == FM_STAGE_B || MODE == FM_STAGE_B_ES)) {
-        hvr = step_ptr<FP16>(sd.hist, ic - 1, nih);
-        if (FP16) {
-          const unsigned* a = sd.amax + (size_t)(ic - 1) * 3 * kAmaxSlots;
-          sc_vx = pow2f(amax_exponent(warp_amax_slots(a + kAmaxSlots)) - 15);
-          sc_vz = pow2f(amax_exponent(warp_amax_slots(a + 2 * kAmaxSlots)) - 15);
-        }
+      if (live && kB && FP16) {
+        const unsigned* a = sd.amax + (size_t)(sd.nt - it) * 3 * kAmaxSlots;
+        sc_vx = pow2f(amax_exponent(warp_amax_slots(a + kAmaxSlots)) - 15);
+        sc_vz = pow2f(amax_exponent(warp_amax_slots(a + 2 * kAmaxSlots)) - 15);
       }
     }
     const int i1 = id.r0 + 2 * lane;
@@ -520,9 +542,8 @@ __global__ void __launch_bounds__(kThreadsT, 2)
     const bool u0 = ok0 && i1 >= 2 && i1 < hi1, u1 = ok1 && i1 + 1 >= 2 && i1 + 1 < hi1;
     const bool r0 = ok0 && i1 >= npml && i1 < npml + g.n1;
     const bool r1 = ok1 && i1 + 1 >= npml && i1 + 1 < npml + g.n1;
-    const int h1 = i1 - npml + (npml & 1);
+    const int h1 = i1 - hbase;
     const int cb = id.c0 + CPT * warp;
-    // ---- global prefetch before waiting for the tile
     float2 d1b = make_float2(0.f, 0.f), bw1 = make_float2(0.f, 0.f);
     if (live) {
       if (ok1) {
@@ -535,7 +556,6 @@ __global__ void __launch_bounds__(kThreadsT, 2)
     }
     float d2b[CPT], bw2[CPT];
     int clo[CPT], chi[CPT];
-    float2 hx[CPT], hz[CPT];
 #pragma unroll
     for (int j = 0; j < CPT; ++j) {
       const int c = cb + j;
@@ -544,19 +564,10 @@ __global__ void __launch_bounds__(kThreadsT, 2)
       bw2[j] = cok ? __ldg(m.bw2 + c) : 0.f;
       clo[j] = (cok && do_inj) ? __ldg(sd.inj.col_lo + c) : 0x7fffffff;
       chi[j] = (cok && do_inj) ? __ldg(sd.inj.col_hi + c) : -1;
-      hx[j] = hz[j] = make_float2(0.f, 0.f);
-      if (MODE == FM_STAGE_B || MODE == FM_STAGE_B_ES) {
-        const int i2p = c - npml;
-        if (cok && i2p >= 0 && i2p < g.n2 && (r0 || r1)) {
-          const int ho = h1 + n1h * i2p;
-          hx[j] = hist_raw<FP16>(hvr, (int)nih + ho, r0, r1);
-          hz[j] = hist_raw<FP16>(hvr, 2 * (int)nih + ho, r0, r1);
-        }
-      }
     }
     bar_wait(&bar[stage], stage ? phase1 : phase0, L.err);
     if (stage) phase1 ^= 1; else phase0 ^= 1;
-    const unsigned char* st = smem + stage * kVStage;
+    const unsigned char* st = smem + stage * kStage;
     const float* P = reinterpret_cast<const float*>(st);  // [TC+3][72]: row 0 = r0-4, col 0 = c0-1
     const float2* P2 = reinterpret_cast<const float2*>(st);
     const float2* VX = reinterpret_cast<const float2*>(st + kVP);
@@ -600,24 +611,26 @@ __global__ void __launch_bounds__(kThreadsT, 2)
             vz_.y = fwd ? fadd(az, bz) : fsub(az, bz);
           }
         }
-        if ((MODE == FM_STAGE_B || MODE == FM_STAGE_B_ES) && cint) {
+        if (kB && cint && (r0 || r1)) {
+          const float2 hx = hist_box_read<FP16>(st + kVStage, cc, lane);
+          const float2 hz = hist_box_read<FP16>(st + kVStage + hist_box(FP16), cc, lane);
           if (r0) {
-            vx_.x = fadd(vx_.x, fmul(fmul(mdt, hx[j].x * sc_vx), 1.0f));
-            vz_.x = fadd(vz_.x, fmul(fmul(mdt, hz[j].x * sc_vz), 1.0f));
+            vx_.x = fadd(vx_.x, fmul(fmul(mdt, hx.x * sc_vx), 1.0f));
+            vz_.x = fadd(vz_.x, fmul(fmul(mdt, hz.x * sc_vz), 1.0f));
           }
           if (r1) {
-            vx_.y = fadd(vx_.y, fmul(fmul(mdt, hx[j].y * sc_vx), 1.0f));
-            vz_.y = fadd(vz_.y, fmul(fmul(mdt, hz[j].y * sc_vz), 1.0f));
+            vx_.y = fadd(vx_.y, fmul(fmul(mdt, hx.y * sc_vx), 1.0f));
+            vz_.y = fadd(vz_.y, fmul(fmul(mdt, hz.y * sc_vz), 1.0f));
           }
         }
         if (i1 + 1 >= clo[j] && i1 <= chi[j]) {  // vz source (type_src = 1)
-          const int base = __ldg(sd.inj.col_base + c);
+          const int base = __ldg(sd.inj.col_base + c) - clo[j];
           if (i1 >= clo[j])
-            vz_.x = inject_at(sd.inj, vz_.x, i1, clo[j], base, dt, 1.0f, sd.amp + (it - 1),
-                              sd.amp_stride, +1);
+            vz_.x = inject_at_global(sd.inj, vz_.x, base + i1, dt, 1.0f, sd.amp + (it - 1),
+                                     sd.amp_stride, +1);
           if (ok1 && i1 + 1 <= chi[j])
-            vz_.y = inject_at(sd.inj, vz_.y, i1 + 1, clo[j], base, dt, 1.0f, sd.amp + (it - 1),
-                              sd.amp_stride, +1);
+            vz_.y = inject_at_global(sd.inj, vz_.y, base + i1 + 1, dt, 1.0f, sd.amp + (it - 1),
+                                     sd.amp_stride, +1);
         }
         if (dst_x) vz_.x = vz_.y;
         *reinterpret_cast<float2*>(sd.vx + k) = vx_;
@@ -647,17 +660,42 @@ __global__ void __launch_bounds__(kThreadsT, 2)
     warp_amax_flush(lmx, a + kAmaxSlots);
     warp_amax_flush(lmz, a + 2 * kAmaxSlots);
   }
+  // receiver / datum gathers (the pressure field is not modified here)
+  if (MODE != FM_STAGE_A) {
+    const int ngb = ngb_per_shot * L.nshots;
+    for (int gb = gridDim.x - 1 - blockIdx.x; gb < ngb; gb += gridDim.x) {
+      const int shot = gb / ngb_per_shot;
+      const ShotDevice& so = L.shots[shot];
+      if (!so.active || it > so.nt || so.type_rec != 0) continue;
+      const int s = (gb % ngb_per_shot) * 8 + warp;
+      if (s < so.rec.n) {
+        if (so.out) {
+          const float v = warp_gather_ordered(prod + warp * 444, so.rec.ix1, so.rec.ix2,
+                                              so.rec.tile, s, so.p, g.ld, 0, g.n1e, g.n2e);
+          const int row = so.out_reverse ? so.nt - it : it - 1;
+          if (lane == 0) so.out[row + (size_t)so.nt * s] = v;
+        }
+      } else if (s - so.rec.n < so.datum.n && so.red &&
+                 (MODE == FM_FWD || MODE == FM_STAGE_B_ES)) {
+        const int d = s - so.rec.n;
+        const float v = warp_gather_ordered(prod + warp * 444, so.datum.ix1, so.datum.ix2,
+                                            so.datum.tile, d,
+                                            so.p + g.npml + (size_t)g.ld * g.npml, g.ld,
+                                            g.npml, g.n1, g.n2);
+        if (lane == 0) so.red[(it - 1) + (size_t)so.nt * d] = v;
+      }
+    }
+  }
 }
 
 template <int MODE>
 void launch_p(const Grid& g, const ModelDev& m, const FusedLaunch& L, int it, cudaStream_t st) {
   const int ntiles = tma_tiles(g) * L.nshots;
   const int grid = std::min(ntiles, L.persist_p);
-  const size_t smem = 2 * kPStage + 16;
   if (L.hist_fp16)
-    k_tma_p<MODE, true><<<grid, kThreadsT, smem, st>>>(g, m, L, it, ntiles);
+    k_tma_p<MODE, true><<<grid, kThreadsT, p_smem(MODE, true), st>>>(g, m, L, it, ntiles);
   else
-    k_tma_p<MODE, false><<<grid, kThreadsT, smem, st>>>(g, m, L, it, ntiles);
+    k_tma_p<MODE, false><<<grid, kThreadsT, p_smem(MODE, false), st>>>(g, m, L, it, ntiles);
 }
 
 template <int MODE>
@@ -666,11 +704,10 @@ void launch_v(const Grid& g, const ModelDev& m, const FusedLaunch& L, int it, cu
   const int stations = (MODE == FM_STAGE_A) ? 0 : L.max_rec + L.max_datum;
   const int ngbps = (stations + 7) / 8;
   const int grid = std::max(1, std::min(std::max(ntiles, ngbps * L.nshots), L.persist_v));
-  const size_t smem = 2 * kVStage + 128 + kGatherBytes;
   if (L.hist_fp16)
-    k_tma_v<MODE, true><<<grid, kThreadsT, smem, st>>>(g, m, L, it, ntiles, ngbps);
+    k_tma_v<MODE, true><<<grid, kThreadsT, v_smem(MODE, true), st>>>(g, m, L, it, ntiles, ngbps);
   else
-    k_tma_v<MODE, false><<<grid, kThreadsT, smem, st>>>(g, m, L, it, ntiles, ngbps);
+    k_tma_v<MODE, false><<<grid, kThreadsT, v_smem(MODE, false), st>>>(g, m, L, it, ntiles, ngbps);
 }
 
 template <typename K>
@@ -683,8 +720,8 @@ int occupancy(K kernel, size_t smem) {
 
 template <int MODE, bool FP16>
 void prep_mode(int* pp, int* pv) {
-  *pp = std::min(*pp, occupancy(k_tma_p<MODE, FP16>, 2 * kPStage + 16));
-  *pv = std::min(*pv, occupancy(k_tma_v<MODE, FP16>, 2 * kVStage + 128 + kGatherBytes));
+  *pp = std::min(*pp, occupancy(k_tma_p<MODE, FP16>, p_smem(MODE, FP16)));
+  *pv = std::min(*pv, occupancy(k_tma_v<MODE, FP16>, v_smem(MODE, FP16)));
 }
 
 }  // namespace
@@ -731,10 +768,12 @@ void tma_v_step(const Grid& g, const ModelDev& m, const FusedLaunch& L, int mode
   }
 }
 
-// Host: the eight 2-D tensor maps of one shot (extended-grid fields,
-// innermost dimension n1e rows with stride ld, n2e columns).
+// Host: the tensor maps of one shot -- 2-D maps of the extended-grid fields
+// (innermost dimension n1e rows with stride ld, n2e columns) and the 3-D map
+// of its history [3*nsteps][n2][n1h] (FP16 or FP32).
 bool tma_encode_maps(const Grid& g, const float* vx, const float* vz, const float* px,
-                     const float* pz, const float* p, const float* kap, TmaMaps* out) {
+                     const float* pz, const float* p, const float* kap, const void* hist,
+                     int hist_fp16, int n1h, int nsteps, TmaMaps* out) {
   static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
   if (!encode) {
     cudaDriverEntryPointQueryResult q;
@@ -755,7 +794,17 @@ bool tma_encode_maps(const Grid& g, const float* vx, const float* vz, const floa
                   CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) ==
            CUDA_SUCCESS;
   };
-  return make(&out->vx19, vx, TR, TC + 3) && make(&out->vz72, vz, TR + 2 * HR, TC) &&
+  const size_t esz = hist_fp16 ? 2 : 4;
+  cuuint64_t hd[3] = {(cuuint64_t)n1h, (cuuint64_t)g.n2, (cuuint64_t)3 * nsteps};
+  cuuint64_t hs[2] = {(cuuint64_t)n1h * esz, (cuuint64_t)n1h * g.n2 * esz};
+  cuuint32_t hb[3] = {(cuuint32_t)TR, (cuuint32_t)TC, 1};
+  cuuint32_t he[3] = {1, 1, 1};
+  const bool ok_hist =
+      encode(&out->hist, hist_fp16 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32,
+             3, const_cast<void*>(hist), hd, hs, hb, he, CU_TENSOR_MAP_INTERLEAVE_NONE,
+             CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_NONE,
+             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+  return ok_hist && make(&out->vx19, vx, TR, TC + 3) && make(&out->vz72, vz, TR + 2 * HR, TC) &&
          make(&out->px, px, TR, TC) && make(&out->pz, pz, TR, TC) &&
          make(&out->p72, p, TR + 2 * HR, TC + 3) && make(&out->vx16, vx, TR, TC) &&
          make(&out->vz16, vz, TR, TC) && make(&out->kap, kap, TR, TC);
