@@ -55,15 +55,21 @@ def make_workload(nt=None):
     return w
 
 
-def shot_dicts(pkg, h, w, shot_ids):
-    """Observed data are modelled in the true model (mode 0) on the GPU."""
+def shot_dicts(pkg, h, w, shot_ids, model_dobs=True):
+    """Observed data are modelled in the true model (mode 0) on the GPU.  The
+    reduced profiling variants use dobs = 0 instead: their records are too
+    short for a reflection to separate the true and background models, and a
+    zero residual would stop MINRES before its first iteration."""
     rec = pkg.subacqui(w.rec_pos[0], w.h, w.npml, w.ofs)
     s = w.wavelet(w.nt)
     h.set_model(w.vtrue, w.npml, w.h, w.dt, w.ofs)
     shots = []
     for i in shot_ids:
         src = pkg.subacqui(w.src_pos[i:i + 1], w.h, w.npml, w.ofs)[0]
-        dobs, _ = h.submodeling(s, src, rec)
+        if model_dobs:
+            dobs, _ = h.submodeling(s, src, rec)
+        else:
+            dobs = np.zeros((w.nt, rec.shape[0]), np.float32, order="F")
         shots.append(dict(s=s, nt=w.nt, src=src, rec=rec, dobs=dobs, mu=w.mu,
                           maxiter=w.maxiter, rtol=0.0, band=w.band, shot=i + 1))
     h.set_model(w.c0, w.npml, w.h, w.dt, w.ofs)
@@ -197,58 +203,54 @@ def roofline(pkg, tim, nshots, w, steps_per_op):
 
 
 def run_ours(args):
-    rank, world = env_int("RANK", 0), env_int("WORLD_SIZE", 1)
-    local = env_int("LOCAL_RANK", 0)
-    dist = None
-    if world > 1:
-        import torch.distributed as dist
-        dist.init_process_group("gloo", timeout=__import__("datetime").timedelta(seconds=600))
     pkg = entry.load_package()
-    w = make_workload()
+    from daw_b200 import ranks
+    rank, world, local = ranks.rank_env()
+    dist = ranks.init_group(world)
+    w = make_workload(args.nt)
+    if args.maxiter is not None:
+        w.maxiter = args.maxiter
     B = args.batch
-    ids = [(rank * B * 7 + k) % 50 for k in range(B)]
+    # this rank's shots: the first B of its para_range block of the 50 shots
+    ids = ranks.rank_shots(len(w.src_pos), B, rank, world)
+    reduced = w.nt != 7500 or w.maxiter != 20  # profiling-sized variant
     h = pkg.Handle(local, preset="mixed")
-    shots = shot_dicts(pkg, h, w, ids)
+    shots = shot_dicts(pkg, h, w, ids, model_dobs=not reduced)
     h.stage_shots(shots)
     for _ in range(args.warmup):
         h.run_staged()
 
-    def barrier():
-        if dist:
-            dist.barrier()
-
     h.reset_timing()
-    barrier()
+    ranks.barrier(dist)
     dev_ms = []
     with Clocks(local) as clk:
         for _ in range(args.steps):
             dev_ms.append(h.run_staged())
-    barrier()
+    ranks.barrier(dist)
     tim = h.timing()
-    total_ms = sum(dev_ms)
-    if dist:
-        import torch
-        t = torch.tensor([total_ms], dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
+    total_ms = ranks.max_over_ranks(dist, sum(dev_ms))
     shots_done = B * args.steps * world
     value = shots_done * 3600.0 / (total_ms * 1e-3)
-    steps_per_op = (2 * (w.nt) + 1 + 2 * w.nt) * (3 + w.maxiter) * args.steps
-    # per op application: stage A (nt steps + flush) + stage B (nt steps)
-    roof = roofline(pkg, tim, B, w, steps_per_op / 2)
+    # G G^T applications per shot: the shift's (1), the reference's unused one
+    # (1) and one per MINRES iteration (rtol 0: all run); each is stage A (nt
+    # steps + the history flush step) followed by stage B (nt steps)
+    op_steps = (2 * w.nt + 1) * (2 + w.maxiter) * args.steps
+    roof = roofline(pkg, tim, B, w, op_steps)
     # accuracy of the mixed path against the FP32-history fused path on the same shots
     out_mixed = h.fetch_staged(outputs=("deltade", "redatumed"))
     # e2e through the public API with host buffers
-    h.reset_timing()
-    t0 = time.perf_counter()
-    outs = h.shots(shots, outputs=("deltade", "redatumed"))
-    e2e_s = time.perf_counter() - t0
-    h_bytes = sum(sh["s"].nbytes + sh["dobs"].nbytes + sh["rec"].nbytes for sh in shots)
-    d_bytes = sum(o["deltade"].nbytes + o["redatumed"].nbytes for o in outs)
+    e2e = None
+    if not args.no_e2e:
+        h.reset_timing()
+        t0 = time.perf_counter()
+        outs = h.shots(shots, outputs=("deltade", "redatumed"))
+        e2e_s = time.perf_counter() - t0
+        h_bytes = sum(sh["s"].nbytes + sh["dobs"].nbytes + sh["rec"].nbytes for sh in shots)
+        d_bytes = sum(o["deltade"].nbytes + o["redatumed"].nbytes for o in outs)
+        e2e = {"value": B * 3600.0 / e2e_s, "unit": "shots/hour",
+               "h2d_bytes_per_step": int(h_bytes), "d2h_bytes_per_step": int(d_bytes)}
     h.close()
     del h
-    e2e = {"value": B * 3600.0 / e2e_s, "unit": "shots/hour",
-           "h2d_bytes_per_step": int(h_bytes), "d2h_bytes_per_step": int(d_bytes)}
     result = None
     plain = None
     if rank == 0 and not args.no_plain:
@@ -270,7 +272,7 @@ def run_ours(args):
                  "mixed_vs_plain_rel_l2": {"redatumed": err_red, "deltade": err_de},
                  "ratio_mixed_over_plain": value / world / (3600.0 / (pms * 1e-3))}
     cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu:
+    if rank == 0 and world == 1 and not args.no_cpu and not reduced:
         print(json.dumps({"partial": True, "value": value, "e2e": e2e, "plain_fp32": plain}),
               file=sys.stderr, flush=True)
         try:
@@ -284,8 +286,10 @@ def run_ours(args):
             "ms_per_step": total_ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32 stencil / f16 history / f64 scalars",
             "data": "synthetic (seeded; observed data modelled in the true model)",
-            "config": {"workload": "751x2301 h=4 m, npml 40, nt 7500 @ 0.4 ms, 576 receivers, "
-                                   "15 Hz, 20 MINRES iterations, datum at 1200 m",
+            "config": {"workload": f"751x2301 h=4 m, npml 40, nt {w.nt} @ 0.4 ms, 576 receivers, "
+                                   f"15 Hz, {w.maxiter} MINRES iterations, datum at 1200 m"
+                                   + (" (reduced profiling variant with dobs = 0, not the "
+                                      "benchmark)" if reduced else ""),
                        "shots_per_step_per_gpu": B, "parallelism": f"shots x{world} (no collective)",
                        "l2": "working set (78 GB FP16 history per shot) far exceeds L2"},
             "clocks": clk.summary(),
@@ -299,7 +303,7 @@ def run_ours(args):
         }
         print(json.dumps(result), flush=True)
     if dist:
-        dist.barrier()
+        ranks.barrier(dist)
         dist.destroy_process_group()
 
 
@@ -338,6 +342,11 @@ def main():
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-procs", type=int, default=None)
+    # profiling variants of the same workload (shorter records / fewer
+    # iterations, same grid and kernels); a line printed with them is marked
+    ap.add_argument("--nt", type=int, default=7500)
+    ap.add_argument("--maxiter", type=int, default=None)
+    ap.add_argument("--no-e2e", action="store_true")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

@@ -62,7 +62,9 @@ enum daw_option {
   DAW_OPT_SKIP_DEAD_OP = 5,  /* 1 = skip MINRES's unused initial operator
                                 application (minresModule.f90:132); default 0 */
   DAW_OPT_MAX_BATCH = 6,     /* upper bound on shots per batched launch (0 = auto) */
-  DAW_OPT_CHUNK = 7          /* fused kernels: columns per thread, 1, 2 or 4 (0 = 2) */
+  DAW_OPT_CHUNK = 7          /* fused kernels: 0 = TMA-pipelined persistent kernels
+                                (default); 1, 2 or 4 = register kernels with that
+                                many columns per thread */
 };
 
 /* Handle lifetime ------------------------------------------------------- */
