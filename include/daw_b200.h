@@ -133,6 +133,27 @@ int daw_wavefield_resample(daw_handle* h, const float* wavefield, int32_t nt,
 int daw_filmartin2d(daw_handle* h, const float* in, int32_t nr, int32_t nt, float dt,
                     float* flow, float* fhig, float* llow, float* lhig, float* out);
 
+/* filmartin2d on traces already in device memory, allocating nothing.  It
+ * has no counterpart in the reference.  It is for callers that cannot
+ * allocate GPU memory at the moment they filter: HBM already held by a shot
+ * batch (admitted up to ~92 % of the device) or by a framework's caching
+ * allocator, or code that must not stall other streams with the device-wide
+ * synchronisation of cudaMalloc/cudaFree.
+ *   d_in, d_out: (nt,nr) column-major float32 device buffers of the current
+ *   device (caller-owned); band parameters in/out as in daw_filmartin2d;
+ *   stream: a cudaStream_t (NULL = legacy default stream); err: optional
+ *   buffer of err_len bytes for the message of a failed call.
+ * Work space is one fixed 4 MiB array that every GPU loading the library
+ * holds until exit (weights for nto <= 65536, FFT space for long traces).
+ * nt above 65536 is rejected with DAW_ERR_ARG.  The first call on a device
+ * takes the array's device address with that device current; make it before
+ * any stream capture.  Calls share the array, so their GPU work must not
+ * overlap: calls are serialised by a lock and return after their work has
+ * finished on `stream`. */
+int daw_filmartin2d_noalloc(const float* d_in, int32_t nr, int32_t nt, float dt, float* flow,
+                            float* fhig, float* llow, float* lhig, float* d_out, void* stream,
+                            char* err, int32_t err_len);
+
 /* Mode-1 DAW shot pipeline (sub_redatum_DAW.f90:73-156) with the mode-2
  * resampling at the datum receivers fused on the fly (:230-240) ---------- */
 typedef struct daw_shot_desc {

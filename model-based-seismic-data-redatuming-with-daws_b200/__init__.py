@@ -110,6 +110,8 @@ def _declare(L):
                                     C.POINTER(MinresInfo)]
     L.daw_wavefield_resample.argtypes = [vp, fp, i32, ip, i32, fp]
     L.daw_filmartin2d.argtypes = [vp, fp, i32, i32, f32, fp, fp, fp, fp, fp]
+    L.daw_filmartin2d_noalloc.argtypes = [vp, i32, i32, f32, fp, fp, fp, fp, vp, vp,
+                                          C.c_char_p, i32]
     L.daw_shot.argtypes = [vp, C.POINTER(ShotDesc), C.POINTER(ShotOut)]
     L.daw_shots.argtypes = [vp, i32, C.POINTER(ShotDesc), C.POINTER(ShotOut)]
     L.daw_stage_shots.argtypes = [vp, i32, C.POINTER(ShotDesc)]

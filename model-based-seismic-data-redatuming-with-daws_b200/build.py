@@ -27,7 +27,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-ffp-contract=off",
           f"-I{INCLUDE}", f"-I{CSRC}"]
 LIB_SOURCES = ["hicks.cpp", "engine.cu", "stencil_plain.cu", "stencil_fused.cu", "stencil_tma.cu", "minres.cu",
-               "filter.cu", "driver.cpp"]
+               "filter.cu", "filter_noalloc.cu", "driver.cpp"]
 
 
 def _needs(out: str, deps: list[str]) -> bool:

@@ -908,23 +908,30 @@ void batch_minres(daw_handle* h, Batch& b) {
 // ---------------------------------------------------------------------------
 namespace {
 
-void hanning_branch(std::vector<float>& han, int nf, int nord) {
+// Element j (1-based, j <= nf + 1) of sphanning's Hanning branch of order
+// nord over nf + 1 points (src/minresModule.f90:619-632).
+float hanning_at(int j, int nf, int nord) {
   const float pi = 3.14159265f;
-  han.resize(nf + 1);
-  for (int j = 1; j <= nf + 1; ++j) {
-    const float a = 2.0f * pi * (float)(j - 1) / (float)(2 * nf);
-    const float b = (std::cos(a) + 1.0f) / 2.0f + 0.000001f;
-    han[j - 1] = std::exp(std::log(b) * (float)nord);
-  }
+  const float a = 2.0f * pi * (float)(j - 1) / (float)(2 * nf);
+  const float b = (std::cos(a) + 1.0f) / 2.0f + 0.000001f;
+  return std::exp(std::log(b) * (float)nord);
 }
 
-// Returns nto; fills w[0..nto] and applies the in-place fhig/lhig clamp.
-int filter_weights(int nt, float dt, float* flow, float* fhig, float* llow, float* lhig,
-                   std::vector<double>& w) {
-  int nto = 0;
+}  // namespace
+
+namespace daw {
+
+int filter_nto(int nt) {
   for (int s = 8; s <= 65536; s *= 2)
-    if (nt <= s) { nto = s; break; }
-  if (nto == 0) throw DawError{DAW_ERR_ARG, "filmartin2d: nt exceeds 65536"};
+    if (nt <= s) return s;
+  return 0;
+}
+
+int filter_weights_into(int nt, float dt, float* flow, float* fhig, float* llow, float* lhig,
+                        float* fm, double* w) {
+  const int nto = filter_nto(nt);
+  if (nto == 0) return 0;
+  std::fill(fm, fm + nto + 1, 0.0f);
   const float fe = 1.0f / dt, fmax = fe / 2.0f;
   if (*fhig > fmax) {
     *fhig = fmax;
@@ -938,20 +945,32 @@ int filter_weights(int nt, float dt, float* flow, float* fhig, float* llow, floa
   int ilhig = (int)(*lhig * (float)conv) + 1;
   if (iflow - illow < 1 && iflow > 0) illow = iflow - 1;
   if (ifhig + ilhig > nto) ilhig = nto - ifhig;
-  std::vector<float> fm(nto + 1, 0.0f), han;
+  // Taper branches: only the taps that land on bins 0..nto are evaluated.
   if (illow > 0) {
-    hanning_branch(han, illow, 2);
-    for (int j = 1; j <= illow; ++j)
-      if (iflow - j >= 0 && iflow - j <= nto) fm[iflow - j] = han[j - 1];
+    const int j0 = std::max(1, iflow - nto), j1 = std::min(illow, iflow);
+    for (int j = j0; j <= j1; ++j) fm[iflow - j] = hanning_at(j, illow, 2);
   }
   if (ilhig > 0) {
-    hanning_branch(han, ilhig, 2);
-    for (int j = 1; j <= ilhig; ++j)
-      if (ifhig + j - 2 >= 0 && ifhig + j - 2 <= nto) fm[ifhig + j - 2] = han[j - 1];
+    const int j0 = std::max(1, 2 - ifhig), j1 = std::min(ilhig, nto + 2 - ifhig);
+    for (int j = j0; j <= j1; ++j) fm[ifhig + j - 2] = hanning_at(j, ilhig, 2);
   }
   for (int j = std::max(iflow, 1); j <= std::min(ifhig, nto + 1); ++j) fm[j - 1] = 1.0f;
-  w.resize(nto + 1);
   for (int j = 0; j <= nto; ++j) w[j] = (double)(fm[j] + 0.0001f);
+  return nto;
+}
+
+}  // namespace daw
+
+namespace {
+
+// Returns nto; fills w[0..nto] and applies the in-place fhig/lhig clamp.
+int filter_weights(int nt, float dt, float* flow, float* fhig, float* llow, float* lhig,
+                   std::vector<double>& w) {
+  const int nto = filter_nto(nt);
+  if (nto == 0) throw DawError{DAW_ERR_ARG, "filmartin2d: nt exceeds 65536"};
+  std::vector<float> fm(nto + 1);
+  w.resize(nto + 1);
+  filter_weights_into(nt, dt, flow, fhig, llow, lhig, fm.data(), w.data());
   return nto;
 }
 

@@ -145,5 +145,13 @@ void vec_add(const float* a, const float* b, float* c, size_t n, cudaStream_t st
 void filter_traces(const float* in, float* out, int nt, int nr, int nto, const double* w,
                    double* scratch, cudaStream_t st);
 size_t filter_scratch_bytes(int nr, int nto);
+// Padded length nto of filmartin2d (next power of two >= nt, 8..65536), or 0
+// when nt exceeds 65536 (src/minresModule.f90:503-510).
+int filter_nto(int nt);
+// The band-pass weights w[0..nto] (src/minresModule.f90:505-586) into caller
+// storage: fm (work) of nto + 1 floats, w of nto + 1 doubles.  Applies the
+// reference's in-place fhig/lhig clamp.  Returns nto, 0 when nt > 65536.
+int filter_weights_into(int nt, float dt, float* flow, float* fhig, float* llow, float* lhig,
+                        float* fm, double* w);
 
 }  // namespace daw
