@@ -38,6 +38,9 @@ sys.path.insert(0, ROOT)
 import __graft_entry__ as entry  # noqa: E402
 
 PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
+# DRAM bytes of one G G^T time step (p + v kernels), measured by ncu on the
+# same grid and batch (profiles/k_tma_751x2301_stageA_stageB.md)
+TRAFFIC = os.path.join(ROOT, "profiles", "k_tma_751x2301_traffic.json")
 METRIC = "shots/hour redatumed at <=1e-3 rel err vs FP64: batched mixed vs plain FP32"
 
 
@@ -195,8 +198,13 @@ def roofline(pkg, tim, nshots, w, steps_per_op):
     launches = steps_per_op
     avg_ms = ms / max(launches, 1)
     achieved = per_step / (avg_ms * 1e-3) / 1e9
+    traffic, traffic_note = None, None
+    if os.path.exists(TRAFFIC):
+        t = json.load(open(TRAFFIC))
+        traffic = t["step_bytes"] * nshots / t["shots_per_launch"]
+        traffic_note = t["note"]
     return {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-            "frac": achieved / peak, "traffic": None,
+            "frac": achieved / peak, "traffic": traffic, "traffic_note": traffic_note,
             "peak_source": "measured" if peaks else "fallback",
             "unit_of_work": "one fused time step (p+v kernels) of the G G^T stages",
             "bytes_per_step": per_step, "avg_step_ms": avg_ms}

@@ -605,7 +605,10 @@ void check_device_error(daw_handle* h) {
   CK(cudaMemcpy(&e, h->d_err, sizeof e, cudaMemcpyDeviceToHost));
   if (e) {
     CK(cudaMemset(h->d_err, 0, sizeof(unsigned)));
-    throw DawError{DAW_ERR_TIMEOUT, "a bounded device wait ran out (TMA tile copy did not complete)"};
+    if (e & kErrTimeout)
+      throw DawError{DAW_ERR_TIMEOUT,
+                     "a bounded device wait ran out (TMA tile copy did not complete)"};
+    throw DawError{DAW_ERR_NAN, "non-finite value (NaN or Inf) in a stage-A wavefield history"};
   }
 }
 
@@ -663,7 +666,7 @@ void run_fused(daw_handle* h, Batch& b, int mode) {
     stop_clock(h, clk, b, mode);
   }
   check_launch("fused steps");
-  if (tma) check_device_error(h);
+  check_device_error(h);
   h->tim.kernel_launches += launches;
   for (ShotCtx* c : b.shots)
     if (c->active) h->tim.point_updates += (double)c->nt * g.n1e * g.n2e;

@@ -23,6 +23,9 @@ namespace daw {
 enum FusedMode { FM_FWD = 0, FM_STAGE_A = 1, FM_STAGE_B = 2, FM_STAGE_B_ES = 3 };
 
 constexpr int kAmaxSlots = 32;  // spread of the max-|x| atomics
+// Bits of the device error flag (FusedLaunch::err).
+constexpr unsigned kErrTimeout = 1u;    // a bounded tile-copy wait ran out
+constexpr unsigned kErrNonFinite = 2u;  // NaN or Inf in a stage-A history field
 
 struct ShotDevice {
   float *px, *pz, *vx, *vz, *p;  // extended-grid state [n2e][ld]

@@ -129,7 +129,11 @@ __device__ __forceinline__ float inject_at(const InjMapDev& m, float v, int i1, 
   return v;
 }
 
-__device__ __forceinline__ void cta_amax(unsigned* red, unsigned v, unsigned* slot) {
+// max |x| as bit patterns of |x| (NaN/Inf rank above every finite value and
+// raise kErrNonFinite)
+__device__ __forceinline__ unsigned abs_bits(float x) { return __float_as_uint(x) & 0x7fffffffu; }
+__device__ __forceinline__ void cta_amax(unsigned* red, unsigned v, unsigned* slot,
+                                         unsigned* err) {
   const unsigned b = __reduce_max_sync(kAll, v);
   if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = b;
   __syncthreads();
@@ -137,6 +141,7 @@ __device__ __forceinline__ void cta_amax(unsigned* red, unsigned v, unsigned* sl
     unsigned r = 0;
     for (int w = 0; w < kWarps; ++w) r = max(r, red[w]);
     if (r) atomicMax(slot, r);
+    if (r >= 0x7f800000u) atomicOr(err, kErrNonFinite);
   }
 }
 
@@ -221,7 +226,7 @@ __global__ void __launch_bounds__(kThreads)
   void* hv_store = (MODE == FM_STAGE_A && it >= 2) ? step_base<FP16>(sd.hist, it - 2, nih) : nullptr;
   const void* hp_read = (MODE == FM_STAGE_B || MODE == FM_STAGE_B_ES)
                             ? step_base<FP16>(sd.hist, ic - 1, nih) : nullptr;
-  float lmax = 0.f;
+  unsigned lmax = 0;
 
 #pragma unroll
   for (int j = 0; j < NP; ++j) {
@@ -301,8 +306,8 @@ __global__ void __launch_bounds__(kThreads)
     st2(pa, k, pv);
     if (cint) {
       if (MODE == FM_STAGE_A) {
-        if (r0) lmax = fmaxf(lmax, fabsf(pv.x));
-        if (r1) lmax = fmaxf(lmax, fabsf(pv.y));
+        if (r0) lmax = max(lmax, abs_bits(pv.x));
+        if (r1) lmax = max(lmax, abs_bits(pv.y));
       }
       if ((MODE == FM_FWD || MODE == FM_STAGE_B_ES) && sd.wf && sd.type_rec == 0) {
         float* w = sd.wf + (size_t)(it - 1) * g.int_elems() + (size_t)g.n1 * i2p;
@@ -318,8 +323,8 @@ __global__ void __launch_bounds__(kThreads)
     }
   }
   if (MODE == FM_STAGE_A && !flush)
-    cta_amax(red, __float_as_uint(lmax),
-             sd.amax + (size_t)(it - 1) * 3 * kAmaxSlots + (blockIdx.x % kAmaxSlots));
+    cta_amax(red, lmax, sd.amax + (size_t)(it - 1) * 3 * kAmaxSlots + (blockIdx.x % kAmaxSlots),
+             L.err);
 }
 
 // ---------------------------------------------------------------------------
@@ -431,7 +436,7 @@ __global__ void __launch_bounds__(kThreads)
   const bool skip_y = fs && i1 + 1 == npml - 1; // row npml-1 written by the next lane
   const bool src_x = fs && i1 == npml;          // also write row npml-1 (previous lane's)
   const bool do_inj = (MODE == FM_FWD) && sd.type_src == 1;
-  float lmx = 0.f, lmz = 0.f;
+  unsigned lmx = 0, lmz = 0;
 #pragma unroll
   for (int j = 0; j < NP; ++j) {
     const int c = t.c0 + j;
@@ -505,19 +510,19 @@ __global__ void __launch_bounds__(kThreads)
       // deferred pressure history of step it (the current p)
       H::put2(hp_store, h1 + n1h * i2p, qp[j + 1].x, qp[j + 1].y, inv_p, r0, r1);
       if (r0) {
-        lmx = fmaxf(lmx, fabsf(vx_.x));
-        lmz = fmaxf(lmz, fabsf(vz_.x));
+        lmx = max(lmx, abs_bits(vx_.x));
+        lmz = max(lmz, abs_bits(vz_.x));
       }
       if (r1) {
-        lmx = fmaxf(lmx, fabsf(vx_.y));
-        lmz = fmaxf(lmz, fabsf(vz_.y));
+        lmx = max(lmx, abs_bits(vx_.y));
+        lmz = max(lmz, abs_bits(vz_.y));
       }
     }
   }
   if (MODE == FM_STAGE_A) {
     unsigned* a = sd.amax + (size_t)(it - 1) * 3 * kAmaxSlots + (blockIdx.x % kAmaxSlots);
-    cta_amax(red[0], __float_as_uint(lmx), a + kAmaxSlots);
-    cta_amax(red[1], __float_as_uint(lmz), a + 2 * kAmaxSlots);
+    cta_amax(red[0], lmx, a + kAmaxSlots, L.err);
+    cta_amax(red[1], lmz, a + 2 * kAmaxSlots, L.err);
   }
 }
 

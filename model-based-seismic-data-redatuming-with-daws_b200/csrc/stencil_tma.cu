@@ -11,11 +11,21 @@
 // reference's separately rounded FP32 operations, and writes its results
 // with coalesced float2 stores.
 //
-// Everything else a tile needs from global memory (the stage-B history
-// stream, the 1-D sponge profiles, the injection bands) is loaded into
-// registers before the CTA waits for the tile, so those latencies overlap the
-// copy; the shot descriptor and the step's FP16 scales are fetched once per
-// shot, not per tile.
+// The 1-D sponge profiles and the injection band bounds of a tile are loaded
+// into registers before the CTA waits for the tile, so those latencies overlap
+// the copy; the shot descriptor and the step's FP16 scales are fetched once
+// per shot, not per tile.
+//
+// Stage A injects the residual at every receiver (441 taps each, summed per
+// grid point in station order).  Tiles crossing that band park their
+// post-stencil pressure pairs in the stage buffer; after a CTA barrier each
+// warp finishes the band rows of its own columns with one lane per row,
+// issuing the row pointers and the tap entries of several points as batches
+// so that the dependent loads overlap.
+//
+// L2 policy: the history stream (written once, read once) is stored and
+// copied with an evict-first hint so it does not push the wavefield state out
+// of L2; the injection tables, re-read every step, are loaded evict-last.
 //
 // Every mbarrier wait is bounded (clock64 budget, ~1 s); on expiry the
 // kernel raises the error flag and continues without hanging.
@@ -43,6 +53,7 @@ constexpr int kVP = 10112;                    // (padded to 128)
 constexpr int kVStage = kVP + 2 * kPF;        // 26496
 constexpr int kGatherBytes = 8 * 444 * 4;     // 14208
 constexpr int kAmpMax = 2048;                 // stations whose amplitudes are staged in smem
+constexpr int kBatch = 6;                     // band-pass entry loads issued per point at once
 constexpr int kAmpBytes = kAmpMax * 4;
 
 // Stage sizes by mode/precision: stage B adds the history box(es) of the
@@ -86,7 +97,7 @@ __device__ __forceinline__ void bar_wait(uint64_t* b, uint32_t parity, unsigned*
   const long long t0 = clock64();
   while (!bar_try(b, parity)) {
     if (clock64() - t0 > (1LL << 31)) {
-      atomicOr(err, 1u);
+      atomicOr(err, kErrTimeout);
       return;
     }
   }
@@ -100,11 +111,11 @@ __device__ __forceinline__ void tma_2d(void* dst, const CUtensorMap* map, int x,
       : "memory");
 }
 __device__ __forceinline__ void tma_3d(void* dst, const CUtensorMap* map, int x, int y, int z,
-                                       uint64_t* b) {
+                                       uint64_t* b, uint64_t pol) {
   asm volatile(
-      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes"
-      " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(smem_u32(dst)),
-      "l"(map), "r"(x), "r"(y), "r"(z), "r"(smem_u32(b))
+      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint"
+      " [%0], [%1, {%2, %3, %4}], [%5], %6;" ::"r"(smem_u32(dst)),
+      "l"(map), "r"(x), "r"(y), "r"(z), "r"(smem_u32(b)), "l"(pol)
       : "memory");
 }
 
@@ -117,9 +128,56 @@ __device__ __forceinline__ float pow2f(int e) { return __int_as_float((e + 127) 
 __device__ __forceinline__ unsigned warp_amax_slots(const unsigned* slots) {
   return __reduce_max_sync(kAll, slots[threadIdx.x & 31]);
 }
-__device__ __forceinline__ void warp_amax_flush(float v, unsigned* slot) {
-  const unsigned b = __reduce_max_sync(kAll, __float_as_uint(v));
-  if ((threadIdx.x & 31) == 0 && b) atomicMax(slot, b);
+// The running max |x| is kept as the bit pattern of |x|: for finite values the
+// integer order is the float order, and NaN/Inf patterns rank above every
+// finite one, so a non-finite value in a history field raises kErrNonFinite.
+__device__ __forceinline__ unsigned abs_bits(float x) { return __float_as_uint(x) & 0x7fffffffu; }
+__device__ __forceinline__ void warp_amax_flush(unsigned v, unsigned* slot, unsigned* err) {
+  const unsigned b = __reduce_max_sync(kAll, v);
+  if ((threadIdx.x & 31) == 0 && b) {
+    atomicMax(slot, b);
+    if (b >= 0x7f800000u) atomicOr(err, kErrNonFinite);
+  }
+}
+
+// L2 eviction priorities.  The history stream (written once in stage A, read
+// once in stage B) is marked evict-first, so that it does not push the
+// wavefield state out of L2; the injection tables, re-read every step, are
+// marked evict-last.
+__device__ __forceinline__ uint64_t l2_evict_first() {
+  uint64_t p;
+  asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+__device__ __forceinline__ uint64_t l2_evict_last() {
+  uint64_t p;
+  asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+__device__ __forceinline__ void st_hint(void* p, uint32_t v, uint64_t pol) {
+  asm volatile("st.global.L2::cache_hint.b32 [%0], %1, %2;" ::"l"(p), "r"(v), "l"(pol) : "memory");
+}
+__device__ __forceinline__ void st_hint(void* p, unsigned short v, uint64_t pol) {
+  asm volatile("st.global.L2::cache_hint.b16 [%0], %1, %2;" ::"l"(p), "h"(v), "l"(pol) : "memory");
+}
+__device__ __forceinline__ void st_hint(void* p, float2 v, uint64_t pol) {
+  asm volatile("st.global.L2::cache_hint.v2.f32 [%0], {%1, %2}, %3;" ::"l"(p), "f"(v.x), "f"(v.y),
+               "l"(pol)
+               : "memory");
+}
+__device__ __forceinline__ float2 ld_hint_f2(const float2* p, uint64_t pol) {
+  float2 v;
+  asm volatile("ld.global.nc.L2::cache_hint.v2.f32 {%0, %1}, [%2], %3;"
+               : "=f"(v.x), "=f"(v.y)
+               : "l"(p), "l"(pol));
+  return v;
+}
+__device__ __forceinline__ int2 ld_hint_i2(const int2* p, uint64_t pol) {
+  int2 v;
+  asm volatile("ld.global.nc.L2::cache_hint.v2.s32 {%0, %1}, [%2], %3;"
+               : "=r"(v.x), "=r"(v.y)
+               : "l"(p), "l"(pol));
+  return v;
 }
 
 template <bool FP16>
@@ -127,14 +185,16 @@ struct Hist;
 template <>
 struct Hist<true> {
   static __device__ __forceinline__ void put2(void* base, int o, float a, float b, float inv,
-                                              bool v0, bool v1) {
+                                              bool v0, bool v1, uint64_t pol) {
     __half* h = static_cast<__half*>(base);
-    if (v0 && v1)
-      *reinterpret_cast<__half2*>(h + o) = __floats2half2_rn(a * inv, b * inv);
-    else if (v0)
-      h[o] = __float2half_rn(a * inv);
-    else if (v1)
-      h[o + 1] = __float2half_rn(b * inv);
+    if (v0 && v1) {
+      const __half2 q = __floats2half2_rn(a * inv, b * inv);
+      st_hint(h + o, *reinterpret_cast<const uint32_t*>(&q), pol);
+    } else if (v0) {
+      st_hint(h + o, __half_as_ushort(__float2half_rn(a * inv)), pol);
+    } else if (v1) {
+      st_hint(h + o + 1, __half_as_ushort(__float2half_rn(b * inv)), pol);
+    }
   }
   static __device__ __forceinline__ float2 get2(const void* base, int o, float sc, bool v0,
                                                 bool v1) {
@@ -149,14 +209,14 @@ struct Hist<true> {
 template <>
 struct Hist<false> {
   static __device__ __forceinline__ void put2(void* base, int o, float a, float b, float,
-                                              bool v0, bool v1) {
+                                              bool v0, bool v1, uint64_t pol) {
     float* h = static_cast<float*>(base);
     if (v0 && v1)
-      *reinterpret_cast<float2*>(h + o) = make_float2(a, b);
+      st_hint(h + o, make_float2(a, b), pol);
     else if (v0)
-      h[o] = a;
+      st_hint(h + o, __float_as_uint(a), pol);
     else if (v1)
-      h[o + 1] = b;
+      st_hint(h + o + 1, __float_as_uint(b), pol);
   }
   static __device__ __forceinline__ float2 get2(const void* base, int o, float, bool v0,
                                                 bool v1) {
@@ -269,7 +329,8 @@ __global__ void __launch_bounds__(kThreadsT, 2)
     tma_2d(st + kPVX + kPVZ + 2 * kPF, &mp->kap, id.r0, id.c0, &bar[s]);
     if (kB) {  // pressure history of the time-reversed step
       const int ic = L.shots[id.shot].nt - it + 1;
-      tma_3d(st + kPStage, &mp->hist, id.r0 - hbase, id.c0 - g.npml, (ic - 1) * 3, &bar[s]);
+      tma_3d(st + kPStage, &mp->hist, id.r0 - hbase, id.c0 - g.npml, (ic - 1) * 3, &bar[s],
+             l2_evict_first());
     }
   };
   int t = blockIdx.x;
@@ -291,7 +352,7 @@ __global__ void __launch_bounds__(kThreadsT, 2)
   bool live = false, flush = false, do_inj = false, amp_smem = false;
   float inv_vx = 1.f, inv_vz = 1.f, sc_p = 1.f;
   void* hvs = nullptr;
-  float lmax = 0.f;
+  unsigned lmax = 0;
   for (; t < ntiles; t += gridDim.x) {
     const int tn = t + gridDim.x;
     if (tid == 0 && tn < ntiles) issue(tn, stage ^ 1);
@@ -299,14 +360,14 @@ __global__ void __launch_bounds__(kThreadsT, 2)
     if (id.shot != cur) {  // CTA-uniform
       if (MODE == FM_STAGE_A && cur >= 0 && live && !flush)
         warp_amax_flush(lmax, sd.amax + (size_t)(it - 1) * 3 * kAmaxSlots +
-                                  ((blockIdx.x * 8 + warp) % kAmaxSlots));
+                                  ((blockIdx.x * 8 + warp) % kAmaxSlots), L.err);
       cur = id.shot;
       sd = L.shots[cur];
       const int nt = sd.nt;
       live = sd.active && (MODE == FM_STAGE_A ? it <= nt + 1 : it <= nt);
       flush = (MODE == FM_STAGE_A) && it == nt + 1;
       do_inj = live && !flush && ((MODE == FM_STAGE_A) || (MODE == FM_FWD && sd.type_src == 0));
-      lmax = 0.f;
+      lmax = 0;
       if (live && MODE == FM_STAGE_A && it >= 2) {
         hvs = step_ptr<FP16>(sd.hist, it - 2, nih);
         if (FP16) {
@@ -332,7 +393,10 @@ __global__ void __launch_bounds__(kThreadsT, 2)
     // ---- global prefetch before waiting for the tile
     float2 d1a = make_float2(0.f, 0.f), d1a1 = make_float2(0.f, 0.f);
     float d2a[CPT], d2a1[CPT];
-    int clo[CPT], chi[CPT];
+    int clo[CPT], chi[CPT];  // forward-source band rows of the thread's columns
+    // Stage A: the receiver band of column cb + lane is held by lane < CPT
+    // (first row, last row, dense-row base) and shuffled out when needed.
+    int bl = 0x7fffffff, bh = -1, bb = 0;
     if (live && !flush) {
       if (ok1) {
         d1a = ldg2(m.d1a + i1);
@@ -348,12 +412,25 @@ __global__ void __launch_bounds__(kThreadsT, 2)
       const bool cok = live && !flush && c < n2e;
       d2a[j] = cok ? __ldg(m.d2a + c) : 0.f;
       d2a1[j] = cok ? __ldg(m.d2a1 + c) : 0.f;
-      clo[j] = (cok && do_inj) ? __ldg(sd.inj.col_lo + c) : 0x7fffffff;
-      chi[j] = (cok && do_inj) ? __ldg(sd.inj.col_hi + c) : -1;
+      clo[j] = (MODE != FM_STAGE_A && cok && do_inj) ? __ldg(sd.inj.col_lo + c) : 0x7fffffff;
+      chi[j] = (MODE != FM_STAGE_A && cok && do_inj) ? __ldg(sd.inj.col_hi + c) : -1;
+    }
+    if (MODE == FM_STAGE_A && do_inj && lane < CPT && cb + lane < n2e) {
+      bl = __ldg(sd.inj.col_lo + cb + lane);
+      bh = __ldg(sd.inj.col_hi + cb + lane);
+      bb = __ldg(sd.inj.col_base + cb + lane);
     }
     bar_wait(&bar[stage], stage ? phase1 : phase0, L.err);
     if (stage) phase1 ^= 1; else phase0 ^= 1;
-    const unsigned char* st = smem + stage * kStage;
+    unsigned park = 0;  // stage A: bit j set when the row pair (i1, i1+1) of column j is in the band
+    if (MODE == FM_STAGE_A) {
+#pragma unroll
+      for (int j = 0; j < CPT; ++j) {
+        const int lo = __shfl_sync(kAll, bl, j), hi = __shfl_sync(kAll, bh, j);
+        if (i1 + 1 >= lo && i1 <= hi) park |= 1u << j;
+      }
+    }
+    unsigned char* st = smem + stage * kStage;
     const float2* VX = reinterpret_cast<const float2*>(st);         // [TC+3][32]
     const float* VZ = reinterpret_cast<const float*>(st + kPVX);    // [TC][72]
     const float2* PX = reinterpret_cast<const float2*>(st + kPVX + kPVZ);
@@ -377,8 +454,9 @@ __global__ void __launch_bounds__(kThreadsT, 2)
         const bool cint = i2p >= 0 && i2p < g.n2;
         if (MODE == FM_STAGE_A && it >= 2 && cint && (r0 || r1)) {
           const int ho = h1 + n1h * i2p;
-          H::put2(hvs, (int)nih + ho, q[j + 2].x, q[j + 2].y, inv_vx, r0, r1);
-          H::put2(hvs, 2 * (int)nih + ho, z.x, z.y, inv_vz, r0, r1);
+          const uint64_t pol = l2_evict_first();
+          H::put2(hvs, (int)nih + ho, q[j + 2].x, q[j + 2].y, inv_vx, r0, r1, pol);
+          H::put2(hvs, 2 * (int)nih + ho, z.x, z.y, inv_vz, r0, r1, pol);
         }
         if (flush) continue;
         float2 px_ = PX[cc * 32 + lane], pz_ = PZ[cc * 32 + lane];
@@ -404,7 +482,15 @@ __global__ void __launch_bounds__(kThreadsT, 2)
             pz_.y = fwd ? fadd(az, bz) : fsub(az, bz);
           }
         }
-        if (i1 + 1 >= clo[j] && i1 <= chi[j]) {  // forward source / stage-A receivers
+        if (MODE == FM_STAGE_A && ((park >> j) & 1u)) {
+          // receiver band: park the post-stencil pair in the stage buffer for
+          // the band pass after this loop
+          *reinterpret_cast<float2*>(sd.pz + k) = pz_;
+          reinterpret_cast<float2*>(st + kPVX + kPVZ)[cc * 32 + lane] = px_;
+          reinterpret_cast<float2*>(st + kPVX + kPVZ + kPF)[cc * 32 + lane] = pz_;
+          continue;
+        }
+        if (i1 + 1 >= clo[j] && i1 <= chi[j]) {  // forward source
           const int base = __ldg(sd.inj.col_base + c) - clo[j];
           const int sg = MODE == FM_FWD ? +1 : -1;
           if (amp_smem) {
@@ -433,8 +519,8 @@ __global__ void __launch_bounds__(kThreadsT, 2)
         *reinterpret_cast<float2*>(sd.p + k) = pv;
         if (cint) {
           if (MODE == FM_STAGE_A) {
-            if (r0) lmax = fmaxf(lmax, fabsf(pv.x));
-            if (r1) lmax = fmaxf(lmax, fabsf(pv.y));
+            if (r0) lmax = max(lmax, abs_bits(pv.x));
+            if (r1) lmax = max(lmax, abs_bits(pv.y));
           }
           if ((MODE == FM_FWD || MODE == FM_STAGE_B_ES) && sd.wf && sd.type_rec == 0) {
             float* w = sd.wf + (size_t)(it - 1) * g.int_elems() + (size_t)g.n1 * i2p;
@@ -450,12 +536,105 @@ __global__ void __launch_bounds__(kThreadsT, 2)
         }
       }
     }
+    if (MODE == FM_STAGE_A) {
+      // Receiver band of this tile: each warp finishes the parked rows of its
+      // own columns, one lane per row.  The row pointers of all its columns
+      // are loaded first, then each point's entries as one batch; the sum
+      // keeps the station order.
+      const int rlast = min(id.r0 + TR, n1e) - 1;
+      const bool wb = lane < CPT && bl <= rlast && bh >= id.r0;
+      if (__syncthreads_or(wb)) {  // CTA-uniform; also orders the parked pairs
+        const float* PXf = reinterpret_cast<const float*>(st + kPVX + kPVZ);
+        const float* PZf = PXf + TR * TC;
+        const float* KAf = PZf + TR * TC;
+        const int2* rp2 = reinterpret_cast<const int2*>(sd.inj.rowptr);
+        for (int pass = 0; pass < TR; pass += 32) {
+          int rr[CPT], e0[CPT], e1[CPT];
+          bool on[CPT];
+#pragma unroll
+          for (int j = 0; j < CPT; ++j) {
+            const int blo = __shfl_sync(kAll, bl, j), bhi = __shfl_sync(kAll, bh, j);
+            const int bbase = __shfl_sync(kAll, bb, j);
+            const int lo = max(blo & ~1, id.r0), hi = min(bhi | 1, rlast);
+            rr[j] = lo + pass + lane;
+            on[j] = blo <= rlast && bhi >= id.r0 && rr[j] <= hi;
+            e0[j] = e1[j] = 0;
+            if (on[j] && rr[j] >= blo && rr[j] <= bhi) {
+              const int2 q = ld_hint_i2(rp2 + bbase + (rr[j] - blo), l2_evict_last());
+              e0[j] = q.x;
+              e1[j] = q.y;
+            }
+          }
+          // Column pairs: the first kBatch entries of the pair's points are
+          // loaded as one batch, their amplitudes looked up once (the source
+          // is CTA-uniform; unused slots hold station 0, a valid index), then
+          // the two chains run interleaved, each in station order.
+          const uint64_t pol = l2_evict_last();
+          const float* amp_g = sd.amp + (it - 1);
+#pragma unroll
+          for (int h = 0; h < CPT; h += 2) {
+            float2 q[2][kBatch];
+#pragma unroll
+            for (int u = 0; u < 2; ++u)
+#pragma unroll
+              for (int k = 0; k < kBatch; ++k)
+                q[u][k] = e0[h + u] + k < e1[h + u] ? ld_hint_f2(sd.inj.ent + e0[h + u] + k, pol)
+                                                    : make_float2(0.f, 0.f);
+            if (amp_smem) {
+#pragma unroll
+              for (int u = 0; u < 2; ++u)
+#pragma unroll
+                for (int k = 0; k < kBatch; ++k) q[u][k].y = amp_s[__float_as_int(q[u][k].y)];
+            } else {
+#pragma unroll
+              for (int u = 0; u < 2; ++u)
+#pragma unroll
+                for (int k = 0; k < kBatch; ++k)
+                  q[u][k].y = __ldg(amp_g + (size_t)__float_as_int(q[u][k].y) * sd.amp_stride);
+            }
+            float v[2], kv[2];
+#pragma unroll
+            for (int u = 0; u < 2; ++u) {
+              const int o = (CPT * warp + h + u) * TR + (rr[h + u] - id.r0);
+              v[u] = on[h + u] ? PXf[o] : 0.f;
+              kv[u] = on[h + u] ? KAf[o] : 0.f;
+            }
+#pragma unroll
+            for (int k = 0; k < kBatch; ++k)
+#pragma unroll
+              for (int u = 0; u < 2; ++u) {
+                const float t = fmul(fmul(fmul(q[u][k].x, dt), q[u][k].y), kv[u]);
+                v[u] = e0[h + u] + k < e1[h + u] ? fsub(v[u], t) : v[u];
+              }
+#pragma unroll
+            for (int u = 0; u < 2; ++u) {
+              const int j = h + u;
+              for (int e = e0[j] + kBatch; e < e1[j]; ++e) {  // more stations than kBatch
+                const float2 q1 = ld_hint_f2(sd.inj.ent + e, pol);
+                const int st1 = __float_as_int(q1.y);
+                const float a1 = amp_smem ? amp_s[st1] : __ldg(amp_g + (size_t)st1 * sd.amp_stride);
+                v[u] = fsub(v[u], fmul(fmul(fmul(q1.x, dt), a1), kv[u]));
+              }
+              if (!on[j]) continue;
+              const int c = cb + j, r = rr[j];
+              const int o = (CPT * warp + j) * TR + (r - id.r0);
+              const float pvv = r < fsrows ? 0.f : fadd(v[u], PZf[o]);
+              const size_t k = (size_t)r + (size_t)ld * c;
+              sd.px[k] = v[u];
+              sd.p[k] = pvv;
+              if (r >= npml && r < npml + g.n1 && c >= npml && c < npml + g.n2)
+                lmax = max(lmax, abs_bits(pvv));
+            }
+          }
+        }
+      }
+    }
     __syncthreads();  // stage buffer (and staged amplitudes) free for reuse
     stage ^= 1;
   }
   if (MODE == FM_STAGE_A && cur >= 0 && live && !flush)
     warp_amax_flush(lmax, sd.amax + (size_t)(it - 1) * 3 * kAmaxSlots +
-                              ((blockIdx.x * 8 + warp) % kAmaxSlots));
+                              ((blockIdx.x * 8 + warp) % kAmaxSlots), L.err);
 }
 
 // ---------------------------------------------------------------------------
@@ -489,9 +668,11 @@ __global__ void __launch_bounds__(kThreadsT, 2)
     tma_2d(st + kVP + kPF, &mp->vz16, id.r0, id.c0, &bar[s]);
     if (kB) {  // velocity histories of the time-reversed step
       const int ic = L.shots[id.shot].nt - it + 1;
-      tma_3d(st + kVStage, &mp->hist, id.r0 - hbase, id.c0 - g.npml, (ic - 1) * 3 + 1, &bar[s]);
+      const uint64_t pol = l2_evict_first();
+      tma_3d(st + kVStage, &mp->hist, id.r0 - hbase, id.c0 - g.npml, (ic - 1) * 3 + 1, &bar[s],
+             pol);
       tma_3d(st + kVStage + hist_box(FP16), &mp->hist, id.r0 - hbase, id.c0 - g.npml,
-             (ic - 1) * 3 + 2, &bar[s]);
+             (ic - 1) * 3 + 2, &bar[s], pol);
     }
   };
   int t = blockIdx.x;
@@ -510,7 +691,7 @@ __global__ void __launch_bounds__(kThreadsT, 2)
   bool live = false, do_inj = false;
   float inv_p = 1.f, sc_vx = 1.f, sc_vz = 1.f;
   void* hps = nullptr;
-  float lmx = 0.f, lmz = 0.f;
+  unsigned lmx = 0, lmz = 0;
   for (; t < ntiles; t += gridDim.x) {
     const int tn = t + gridDim.x;
     if (tid == 0 && tn < ntiles) issue(tn, stage ^ 1);
@@ -518,14 +699,14 @@ __global__ void __launch_bounds__(kThreadsT, 2)
     if (id.shot != cur) {
       if (MODE == FM_STAGE_A && cur >= 0 && live) {
         unsigned* a = sd.amax + (size_t)(it - 1) * 3 * kAmaxSlots + ((blockIdx.x * 8 + warp) % kAmaxSlots);
-        warp_amax_flush(lmx, a + kAmaxSlots);
-        warp_amax_flush(lmz, a + 2 * kAmaxSlots);
+        warp_amax_flush(lmx, a + kAmaxSlots, L.err);
+        warp_amax_flush(lmz, a + 2 * kAmaxSlots, L.err);
       }
       cur = id.shot;
       sd = L.shots[cur];
       live = sd.active && it <= sd.nt;
       do_inj = live && (MODE == FM_FWD) && sd.type_src == 1;
-      lmx = lmz = 0.f;
+      lmx = lmz = 0;
       if (live && MODE == FM_STAGE_A) {
         hps = step_ptr<FP16>(sd.hist, it - 1, nih);
         if (FP16)
@@ -640,14 +821,14 @@ __global__ void __launch_bounds__(kThreadsT, 2)
           *reinterpret_cast<float2*>(sd.vz + k) = vz_;
         if (src_x) sd.vz[k - 1] = vz_.x;
         if (MODE == FM_STAGE_A && cint && (r0 || r1)) {
-          Hist<FP16>::put2(hps, h1 + n1h * i2p, pc.x, pc.y, inv_p, r0, r1);
+          Hist<FP16>::put2(hps, h1 + n1h * i2p, pc.x, pc.y, inv_p, r0, r1, l2_evict_first());
           if (r0) {
-            lmx = fmaxf(lmx, fabsf(vx_.x));
-            lmz = fmaxf(lmz, fabsf(vz_.x));
+            lmx = max(lmx, abs_bits(vx_.x));
+            lmz = max(lmz, abs_bits(vz_.x));
           }
           if (r1) {
-            lmx = fmaxf(lmx, fabsf(vx_.y));
-            lmz = fmaxf(lmz, fabsf(vz_.y));
+            lmx = max(lmx, abs_bits(vx_.y));
+            lmz = max(lmz, abs_bits(vz_.y));
           }
         }
       }
@@ -657,8 +838,8 @@ __global__ void __launch_bounds__(kThreadsT, 2)
   }
   if (MODE == FM_STAGE_A && cur >= 0 && live) {
     unsigned* a = sd.amax + (size_t)(it - 1) * 3 * kAmaxSlots + ((blockIdx.x * 8 + warp) % kAmaxSlots);
-    warp_amax_flush(lmx, a + kAmaxSlots);
-    warp_amax_flush(lmz, a + 2 * kAmaxSlots);
+    warp_amax_flush(lmx, a + kAmaxSlots, L.err);
+    warp_amax_flush(lmz, a + 2 * kAmaxSlots, L.err);
   }
   // receiver / datum gathers (the pressure field is not modified here)
   if (MODE != FM_STAGE_A) {

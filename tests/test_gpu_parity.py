@@ -274,3 +274,20 @@ def test_errors_are_reported(pkg, case):
         assert e.value.code == -1
         with pytest.raises(pkg.DawError):
             h.set_options(preset=3)
+
+
+@pytest.mark.parametrize("opt", [{}, {"chunk": 2}, {"history": 0}])
+def test_non_finite_history_is_reported(pkg, case, opt):
+    """A NaN in the residual reaches the stage-A histories; the fused paths
+    report DAW_ERR_NAN from their max-|x| reduction, and the handle stays
+    usable afterwards."""
+    w = case["w"]
+    res = np.zeros((w.nt, case["rec"].shape[0]), np.float32, order="F")
+    res[7, 3] = np.nan
+    with handle(pkg, case, preset="mixed", **opt) as h:
+        with pytest.raises(pkg.DawError) as e:
+            h.submodeling_adjoint_esource_data(res, case["rec"])
+        assert e.value.code == -5, str(e.value)
+        res[7, 3] = 1.0
+        g = h.submodeling_adjoint_esource_data(res, case["rec"])
+        assert np.isfinite(g).all() and np.abs(g).max() > 0
