@@ -143,6 +143,7 @@ struct ShotCtx {
   float *d_deltade = nullptr, *d_dataesc = nullptr, *d_datae = nullptr;
   float *d_redF = nullptr, *d_redE = nullptr, *d_red = nullptr, *d_redf = nullptr;
   float* d_wf = nullptr;
+  float* d_ampT = nullptr;  // stage-A residual in step-major order [nt][nr]
   // simulation state
   float *px = nullptr, *pz = nullptr, *vx = nullptr, *vz = nullptr, *p = nullptr;
   void* hist = nullptr;
@@ -585,7 +586,7 @@ void fill_shot_devices(daw_handle* h, Batch& b, int mode) {
 }
 
 FusedLaunch launch_of(daw_handle* h, Batch& b) {
-  FusedLaunch L;
+  FusedLaunch L{};  // nparam = 0: no per-shot parameters unless set
   L.shots = b.d_shots;
   L.nshots = (int)b.shots.size();
   L.hist_fp16 = h->opt.history_fp16;
@@ -627,6 +628,19 @@ void stop_clock(daw_handle* h, SimClock& clk, Batch& b, int mode) {
 void run_fused(daw_handle* h, Batch& b, int mode) {
   const Grid& g = h->g;
   FusedLaunch L = launch_of(h, b);
+  L.nparam = std::min<int>((int)b.shots.size(), FusedLaunch::kParamShots);
+  unsigned long long phash = 1469598103934665603ull;  // FNV-1a of the per-shot parameters
+  auto mix = [&](unsigned long long v) { phash = (phash ^ v) * 1099511628211ull; };
+  for (int i = 0; i < FusedLaunch::kParamShots; ++i) {
+    const ShotCtx* c = i < L.nparam ? b.shots[i] : nullptr;
+    L.shot_amax[i] = c ? c->amax : nullptr;
+    L.shot_amp[i] = !c ? nullptr : mode == FM_FWD ? c->d_s : mode == FM_STAGE_A ? c->d_ampT : nullptr;
+    L.shot_nt[i] = c ? c->nt : 0;
+    L.shot_nsta[i] = !c ? 0 : mode == FM_FWD ? 1 : mode == FM_STAGE_A ? c->nr : 0;
+    mix((unsigned long long)(uintptr_t)L.shot_amax[i]);
+    mix((unsigned long long)(uintptr_t)L.shot_amp[i]);
+    mix((unsigned long long)L.shot_nt[i] << 32 | (unsigned)L.shot_nsta[i]);
+  }
   const int last = (mode == FM_STAGE_A) ? b.max_nt + 1 : b.max_nt;  // +1: history flush
   const bool tma = L.chunk == 0;
   auto body = [&]() {
@@ -643,9 +657,9 @@ void run_fused(daw_handle* h, Batch& b, int mode) {
   const long long launches = 2LL * b.max_nt + (mode == FM_STAGE_A ? 1 : 0);
   if (h->opt.graph) {
     char key[256];
-    std::snprintf(key, sizeof key, "m%d.n%d.s%zu.p%p.q%p.c%d.f%d.r%d.d%d", mode, b.max_nt,
+    std::snprintf(key, sizeof key, "m%d.n%d.s%zu.p%p.q%p.c%d.f%d.r%d.d%d.h%llx", mode, b.max_nt,
                   b.shots.size(), (void*)b.d_shots, (void*)b.d_maps, L.chunk, L.hist_fp16,
-                  L.max_rec, L.max_datum);
+                  L.max_rec, L.max_datum, phash);
     auto it = h->graphs.find(key);
     if (it == h->graphs.end()) {
       cudaGraph_t graph;
@@ -721,6 +735,11 @@ void batch_operator(daw_handle* h, Batch& b, bool esource) {
     zero_state(h, *c);
   }
   clear_amax(h, b);
+  for (ShotCtx* c : b.shots)  // step-major residual for the fused kernels' amplitude staging
+    if (c->active && c->nr > 0) {
+      transpose_traces(c->op_in, c->d_ampT, c->nt, c->nr, h->st);
+      h->tim.kernel_launches += 1;
+    }
   fill_shot_devices(h, b, FM_STAGE_A);
   run_fused(h, b, FM_STAGE_A);
   for (ShotCtx* c : b.shots) {
@@ -1043,6 +1062,7 @@ void prepare_shot(daw_handle* h, ShotCtx& c, const daw_shot_desc& d, int slot, b
   c.src = make_stations(h, h->pool, p + "src", s5, 1);
   c.srcmap = make_map(h, h->pool, p + "srcmap", s5, 1);
   c.d_wf = want_wf ? h->pool.get_t<float>(p + "wf", g.int_elems() * (size_t)d.nt) : nullptr;
+  c.d_ampT = h->pool.get_t<float>(p + "ampT", std::max<size_t>(n, 1));
   alloc_state(h, c, slot, d.nt, fp16);
 }
 
@@ -1206,6 +1226,7 @@ ShotCtx& single_ctx(daw_handle* h, ShotCtx& c, int nt, const int32_t* ir, int nr
   c.rec = make_stations(h, h->pool, p + "rec", ir, nr);
   c.recmap = make_map(h, h->pool, p + "recmap", ir, nr);
   c.d_wf = want_wf ? h->pool.get_t<float>(p + "wf", h->g.int_elems() * (size_t)nt) : nullptr;
+  c.d_ampT = h->pool.get_t<float>(p + "ampT", std::max<size_t>(n, 1));
   alloc_state(h, c, 0, nt, h->opt.history_fp16 != 0 && h->opt.fused != 0);
   return c;
 }

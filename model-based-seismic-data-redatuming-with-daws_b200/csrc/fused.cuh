@@ -63,6 +63,17 @@ struct FusedLaunch {
   const TmaMaps* maps;      // device array, one per shot (TMA kernels)
   unsigned* err;            // raised by a bounded wait that ran out
   int persist_p, persist_v; // persistent grid sizes of the TMA kernels
+  // Per-shot pointers passed as kernel parameters for the first kParamShots
+  // shots, so that a CTA's per-shot set-up needs one round of loads: the
+  // max-|x| slots, the injection amplitudes in step-major order
+  // [step][station] (the wavelet, or the transposed residual in stage A), the
+  // record length and the station count of the injection.
+  static constexpr int kParamShots = 8;
+  int nparam;
+  const unsigned* shot_amax[kParamShots];
+  const float* shot_amp[kParamShots];
+  int shot_nt[kParamShots];
+  int shot_nsta[kParamShots];
 };
 
 // TMA kernels (stencil_tma.cu)

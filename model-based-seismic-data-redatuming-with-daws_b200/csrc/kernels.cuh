@@ -138,6 +138,8 @@ int minres_blocks(size_t n);
 void residuals(const float* dobs, const float* datar, float* deltadr, int nt, int nr,
                cudaStream_t st);
 void vec_add(const float* a, const float* b, float* c, size_t n, cudaStream_t st);
+// Traces (nt, nr), time fastest, to step-major [nt][nr] (minres.cu).
+void transpose_traces(const float* in, float* out, int nt, int nr, cudaStream_t st);
 
 // filmartin2d on the device (filter.cu): weights w[0..nto] as the reference
 // builds them; each trace zero padded to nto, FP64 real FFT, bins 0..nto/2-1

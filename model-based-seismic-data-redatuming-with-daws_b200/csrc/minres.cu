@@ -289,6 +289,22 @@ __global__ void k_add(const float* a, const float* b, float* c, size_t n) {
     c[i] = __fadd_rn(a[i], b[i]);
 }
 
+// out[t * nr + r] = in[t + nt * r]: traces (nt, nr) to step-major order, by
+// 32 x 32 tiles through shared memory (both sides coalesced).
+__global__ void k_transpose(const float* __restrict__ in, float* __restrict__ out, int nt, int nr) {
+  __shared__ float tile[32][33];
+  const int t0 = blockIdx.x * 32, r0 = blockIdx.y * 32;
+  for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+    const int t = t0 + threadIdx.x, r = r0 + k;
+    if (t < nt && r < nr) tile[k][threadIdx.x] = in[t + (size_t)nt * r];
+  }
+  __syncthreads();
+  for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+    const int t = t0 + k, r = r0 + threadIdx.x;
+    if (t < nt && r < nr) out[(size_t)t * nr + r] = tile[threadIdx.x][k];
+  }
+}
+
 int grid_for(size_t n) {
   size_t b = (n + 1023) / 1024;
   if (b < 1) b = 1;
@@ -368,6 +384,12 @@ void residuals(const float* dobs, const float* datar, float* deltadr, int nt, in
 
 void vec_add(const float* a, const float* b, float* c, size_t n, cudaStream_t st) {
   k_add<<<grid_for(n), 256, 0, st>>>(a, b, c, n);
+}
+
+void transpose_traces(const float* in, float* out, int nt, int nr, cudaStream_t st) {
+  if (nt <= 0 || nr <= 0) return;
+  const dim3 grid((nt + 31) / 32, (nr + 31) / 32);
+  k_transpose<<<grid, dim3(32, 8), 0, st>>>(in, out, nt, nr);
 }
 
 }  // namespace daw

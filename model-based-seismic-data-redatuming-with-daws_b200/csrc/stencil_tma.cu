@@ -266,6 +266,21 @@ struct TileId {
   int shot, r0, c0;
 };
 
+// The tiles a persistent CTA walks: first, stride, end (exclusive).  With at
+// least one CTA per shot the grid is split into equal groups, one per shot,
+// each walking its shot's tiles round robin, so a CTA sets up one shot only
+// (CTAs left over from the split walk none); otherwise all tiles round robin.
+struct Walk {
+  int t0, stride, end;
+};
+__device__ __forceinline__ Walk tile_walk(int ntiles, int nshots) {
+  const int cps = gridDim.x / nshots;
+  if (cps == 0) return Walk{(int)blockIdx.x, (int)gridDim.x, ntiles};
+  const int sh = blockIdx.x / cps, tps = ntiles / nshots;
+  if (sh >= nshots) return Walk{0, 1, 0};
+  return Walk{sh * tps + (int)blockIdx.x % cps, cps, (sh + 1) * tps};
+}
+
 __device__ __forceinline__ TileId tile_id(const Grid& g, int t) {
   const int nrb = (g.n1e + TR - 1) / TR, ncb = (g.n2e + TC - 1) / TC;
   const int tps = nrb * ncb;
@@ -333,8 +348,9 @@ __global__ void __launch_bounds__(kThreadsT, 2)
              l2_evict_first());
     }
   };
-  int t = blockIdx.x;
-  if (tid == 0 && t < ntiles) issue(t, 0);
+  const Walk wk = tile_walk(ntiles, L.nshots);
+  int t = wk.t0;
+  if (tid == 0 && t < wk.end) issue(t, 0);
   uint32_t phase0 = 0, phase1 = 0;
   int stage = 0;
   const int ld = g.ld, n1e = g.n1e, n2e = g.n2e, npml = g.npml;
@@ -353,33 +369,74 @@ __global__ void __launch_bounds__(kThreadsT, 2)
   float inv_vx = 1.f, inv_vz = 1.f, sc_p = 1.f;
   void* hvs = nullptr;
   unsigned lmax = 0;
-  for (; t < ntiles; t += gridDim.x) {
-    const int tn = t + gridDim.x;
-    if (tid == 0 && tn < ntiles) issue(tn, stage ^ 1);
+  for (; t < wk.end; t += wk.stride) {
+    const int tn = t + wk.stride;
+    if (tid == 0 && tn < wk.end) issue(tn, stage ^ 1);
     const TileId id = tile_id(g, t);
     if (id.shot != cur) {  // CTA-uniform
       if (MODE == FM_STAGE_A && cur >= 0 && live && !flush)
         warp_amax_flush(lmax, sd.amax + (size_t)(it - 1) * 3 * kAmaxSlots +
                                   ((blockIdx.x * 8 + warp) % kAmaxSlots), L.err);
       cur = id.shot;
-      sd = L.shots[cur];
-      const int nt = sd.nt;
-      live = sd.active && (MODE == FM_STAGE_A ? it <= nt + 1 : it <= nt);
-      flush = (MODE == FM_STAGE_A) && it == nt + 1;
-      do_inj = live && !flush && ((MODE == FM_STAGE_A) || (MODE == FM_FWD && sd.type_src == 0));
-      lmax = 0;
-      if (live && MODE == FM_STAGE_A && it >= 2) {
-        hvs = step_ptr<FP16>(sd.hist, it - 2, nih);
-        if (FP16) {
-          const unsigned* a = sd.amax + (size_t)(it - 2) * 3 * kAmaxSlots;
-          inv_vx = pow2f(15 - amax_exponent(warp_amax_slots(a + kAmaxSlots)));
-          inv_vz = pow2f(15 - amax_exponent(warp_amax_slots(a + 2 * kAmaxSlots)));
+      if (cur < L.nparam) {
+        // one round of independent loads: scale slots, amplitudes, descriptor
+        const int ntc = L.shot_nt[cur], nsta = L.shot_nsta[cur];
+        const unsigned* am = L.shot_amax[cur];
+        unsigned s0v = 0, s1v = 0;
+        if (MODE == FM_STAGE_A && FP16 && it >= 2 && it <= ntc + 1) {
+          s0v = am[(size_t)(it - 2) * 3 * kAmaxSlots + kAmaxSlots + lane];
+          s1v = am[(size_t)(it - 2) * 3 * kAmaxSlots + 2 * kAmaxSlots + lane];
         }
+        if (kB && FP16 && it <= ntc) s0v = am[(size_t)(ntc - it) * 3 * kAmaxSlots + lane];
+        constexpr int kPer = kAmpMax / kThreadsT;
+        float av[kPer];
+        const bool want_amps = (MODE == FM_STAGE_A || MODE == FM_FWD) && it <= ntc &&
+                               nsta <= kAmpMax && L.shot_amp[cur] != nullptr;
+#pragma unroll
+        for (int k = 0; k < kPer; ++k) {
+          const int s = tid + k * kThreadsT;
+          av[k] = (want_amps && s < nsta) ? __ldg(L.shot_amp[cur] + (size_t)(it - 1) * nsta + s) : 0.f;
+        }
+        sd = L.shots[cur];
+        live = sd.active && (MODE == FM_STAGE_A ? it <= ntc + 1 : it <= ntc);
+        flush = (MODE == FM_STAGE_A) && it == ntc + 1;
+        do_inj = live && !flush && ((MODE == FM_STAGE_A) || (MODE == FM_FWD && sd.type_src == 0));
+        lmax = 0;
+        if (live && MODE == FM_STAGE_A && it >= 2) {
+          hvs = step_ptr<FP16>(sd.hist, it - 2, nih);
+          if (FP16) {
+            inv_vx = pow2f(15 - amax_exponent(__reduce_max_sync(kAll, s0v)));
+            inv_vz = pow2f(15 - amax_exponent(__reduce_max_sync(kAll, s1v)));
+          }
+        }
+        if (live && kB && FP16) sc_p = pow2f(amax_exponent(__reduce_max_sync(kAll, s0v)) - 15);
+        amp_smem = nsta <= kAmpMax;
+        if (do_inj && amp_smem) {  // CTA-uniform
+#pragma unroll
+          for (int k = 0; k < kPer; ++k)
+            if (tid + k * kThreadsT < nsta) amp_s[tid + k * kThreadsT] = av[k];
+          __syncthreads();
+        }
+      } else {
+        sd = L.shots[cur];
+        const int nt = sd.nt;
+        live = sd.active && (MODE == FM_STAGE_A ? it <= nt + 1 : it <= nt);
+        flush = (MODE == FM_STAGE_A) && it == nt + 1;
+        do_inj = live && !flush && ((MODE == FM_STAGE_A) || (MODE == FM_FWD && sd.type_src == 0));
+        lmax = 0;
+        if (live && MODE == FM_STAGE_A && it >= 2) {
+          hvs = step_ptr<FP16>(sd.hist, it - 2, nih);
+          if (FP16) {
+            const unsigned* a = sd.amax + (size_t)(it - 2) * 3 * kAmaxSlots;
+            inv_vx = pow2f(15 - amax_exponent(warp_amax_slots(a + kAmaxSlots)));
+            inv_vz = pow2f(15 - amax_exponent(warp_amax_slots(a + 2 * kAmaxSlots)));
+          }
+        }
+        if (live && kB && FP16)
+          sc_p = pow2f(amax_exponent(warp_amax_slots(sd.amax + (size_t)(nt - it) * 3 * kAmaxSlots)) - 15);
+        amp_smem = sd.inj.nsta <= kAmpMax;
+        if (do_inj && amp_smem) stage_amp(amp_s, sd.amp + (it - 1), sd.amp_stride, sd.inj.nsta);
       }
-      if (live && kB && FP16)
-        sc_p = pow2f(amax_exponent(warp_amax_slots(sd.amax + (size_t)(nt - it) * 3 * kAmaxSlots)) - 15);
-      amp_smem = sd.inj.nsta <= kAmpMax;
-      if (do_inj && amp_smem) stage_amp(amp_s, sd.amp + (it - 1), sd.amp_stride, sd.inj.nsta);
     }
     const int i1 = id.r0 + 2 * lane;
     const bool ok0 = i1 < n1e, ok1 = i1 + 1 < n1e;
@@ -675,8 +732,9 @@ __global__ void __launch_bounds__(kThreadsT, 2)
              (ic - 1) * 3 + 2, &bar[s], pol);
     }
   };
-  int t = blockIdx.x;
-  if (tid == 0 && t < ntiles) issue(t, 0);
+  const Walk wk = tile_walk(ntiles, L.nshots);
+  int t = wk.t0;
+  if (tid == 0 && t < wk.end) issue(t, 0);
   uint32_t phase0 = 0, phase1 = 0;
   int stage = 0;
   const int ld = g.ld, n1e = g.n1e, n2e = g.n2e, npml = g.npml;
@@ -692,9 +750,9 @@ __global__ void __launch_bounds__(kThreadsT, 2)
   float inv_p = 1.f, sc_vx = 1.f, sc_vz = 1.f;
   void* hps = nullptr;
   unsigned lmx = 0, lmz = 0;
-  for (; t < ntiles; t += gridDim.x) {
-    const int tn = t + gridDim.x;
-    if (tid == 0 && tn < ntiles) issue(tn, stage ^ 1);
+  for (; t < wk.end; t += wk.stride) {
+    const int tn = t + wk.stride;
+    if (tid == 0 && tn < wk.end) issue(tn, stage ^ 1);
     const TileId id = tile_id(g, t);
     if (id.shot != cur) {
       if (MODE == FM_STAGE_A && cur >= 0 && live) {
@@ -703,6 +761,19 @@ __global__ void __launch_bounds__(kThreadsT, 2)
         warp_amax_flush(lmz, a + 2 * kAmaxSlots, L.err);
       }
       cur = id.shot;
+      // scale slots loaded together with the descriptor when the shot's
+      // pointers are kernel parameters
+      unsigned s0v = 0, s1v = 0;
+      const bool fast = cur < L.nparam;
+      if (fast && FP16) {
+        const int ntc = L.shot_nt[cur];
+        const unsigned* am = L.shot_amax[cur];
+        if (MODE == FM_STAGE_A && it <= ntc) s0v = am[(size_t)(it - 1) * 3 * kAmaxSlots + lane];
+        if (kB && it <= ntc) {
+          s0v = am[(size_t)(ntc - it) * 3 * kAmaxSlots + kAmaxSlots + lane];
+          s1v = am[(size_t)(ntc - it) * 3 * kAmaxSlots + 2 * kAmaxSlots + lane];
+        }
+      }
       sd = L.shots[cur];
       live = sd.active && it <= sd.nt;
       do_inj = live && (MODE == FM_FWD) && sd.type_src == 1;
@@ -710,12 +781,16 @@ __global__ void __launch_bounds__(kThreadsT, 2)
       if (live && MODE == FM_STAGE_A) {
         hps = step_ptr<FP16>(sd.hist, it - 1, nih);
         if (FP16)
-          inv_p = pow2f(15 - amax_exponent(warp_amax_slots(sd.amax + (size_t)(it - 1) * 3 * kAmaxSlots)));
+          inv_p = pow2f(15 - amax_exponent(
+                                 fast ? __reduce_max_sync(kAll, s0v)
+                                      : warp_amax_slots(sd.amax + (size_t)(it - 1) * 3 * kAmaxSlots)));
       }
       if (live && kB && FP16) {
         const unsigned* a = sd.amax + (size_t)(sd.nt - it) * 3 * kAmaxSlots;
-        sc_vx = pow2f(amax_exponent(warp_amax_slots(a + kAmaxSlots)) - 15);
-        sc_vz = pow2f(amax_exponent(warp_amax_slots(a + 2 * kAmaxSlots)) - 15);
+        sc_vx = pow2f(amax_exponent(fast ? __reduce_max_sync(kAll, s0v)
+                                         : warp_amax_slots(a + kAmaxSlots)) - 15);
+        sc_vz = pow2f(amax_exponent(fast ? __reduce_max_sync(kAll, s1v)
+                                         : warp_amax_slots(a + 2 * kAmaxSlots)) - 15);
       }
     }
     const int i1 = id.r0 + 2 * lane;
