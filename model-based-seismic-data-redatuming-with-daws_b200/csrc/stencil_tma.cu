@@ -31,6 +31,8 @@
 // kernel raises the error flag and continues without hanging.
 #include <cuda.h>
 
+#include <type_traits>
+
 #include "fused.cuh"
 
 namespace daw {
@@ -266,6 +268,21 @@ struct TileId {
   int shot, r0, c0;
 };
 
+// True when no boundary of the stencil passes crosses the tile: all its rows
+// and columns are updated (away from the grid edge), physical (inside the
+// PML frame), below the free surface rows and, for the final esource, inside
+// the source range [slo, shi).
+__device__ __forceinline__ bool tile_interior(const Grid& g, const TileId& id, int mode, int slo,
+                                              int shi1, int shi2) {
+  const int off = (mode == FM_FWD) ? 2 : 3;
+  const int fsrows = g.ofs == 1 ? g.npml + 1 : 0;
+  const int rlo = max(max(2, g.npml + slo), fsrows);
+  const int rhi = min(min(g.n1e - off, g.npml + shi1), g.n1e);
+  const int clo = max(2, g.npml + slo);
+  const int chi = min(min(g.n2e - off, g.npml + shi2), g.n2e);
+  return id.r0 >= rlo && id.r0 + TR <= rhi && id.c0 >= clo && id.c0 + TC <= chi;
+}
+
 // The tiles a persistent CTA walks: first, stride, end (exclusive).  With at
 // least one CTA per shot the grid is split into equal groups, one per shot,
 // each walking its shot's tiles round robin, so a CTA sets up one shot only
@@ -493,106 +510,118 @@ __global__ void __launch_bounds__(kThreadsT, 2)
     const float2* PX = reinterpret_cast<const float2*>(st + kPVX + kPVZ);
     const float2* PZ = PX + TR * TC / 2;
     const float2* KA = PZ + TR * TC / 2;
-    if (live && ok0) {
-      float2 q[CPT + 3];  // vx at columns cb-2 .. cb+CPT
-#pragma unroll
-      for (int k = 0; k < CPT + 3; ++k) q[k] = VX[(CPT * warp + k) * 32 + lane];
-#pragma unroll
-      for (int j = 0; j < CPT; ++j) {
-        const int cc = CPT * warp + j;
-        const int c = id.c0 + cc;
-        if (c >= n2e) continue;
-        const int k = i1 + ld * c;
-        const float* vzc = VZ + cc * (TR + 2 * HR) + 2 * lane;  // row i1-4
-        const float2 zm = *reinterpret_cast<const float2*>(vzc + 2);
-        const float2 z = *reinterpret_cast<const float2*>(vzc + 4);
-        const float zp2 = vzc[6];
-        const int i2p = c - npml;
-        const bool cint = i2p >= 0 && i2p < g.n2;
-        if (MODE == FM_STAGE_A && it >= 2 && cint && (r0 || r1)) {
-          const int ho = h1 + n1h * i2p;
-          const uint64_t pol = l2_evict_first();
-          H::put2(hvs, (int)nih + ho, q[j + 2].x, q[j + 2].y, inv_vx, r0, r1, pol);
-          H::put2(hvs, 2 * (int)nih + ho, z.x, z.y, inv_vz, r0, r1, pol);
-        }
-        if (flush) continue;
-        float2 px_ = PX[cc * 32 + lane], pz_ = PZ[cc * 32 + lane];
-        const float2 kv = KA[cc * 32 + lane];
-        if (c >= 2 && c < hi2) {
-          const bool fwd = (MODE != FM_STAGE_A);
-          if (u0) {
-            const float der2 = dminus(q[j].x, q[j + 1].x, q[j + 2].x, q[j + 3].x);
-            const float der1 = dminus(zm.x, zm.y, z.x, z.y);
-            const float kd = fmul(dtdx, kv.x);
-            const float ax = fmul(d2a[j], px_.x), bx = fmul(fmul(kd, d2a1[j]), der2);
-            const float az = fmul(d1a.x, pz_.x), bz = fmul(fmul(kd, d1a1.x), der1);
-            px_.x = fwd ? fadd(ax, bx) : fsub(ax, bx);
-            pz_.x = fwd ? fadd(az, bz) : fsub(az, bz);
+    // The stencil pass, compiled twice: for interior tiles (no grid edge, PML
+    // row/column edge, free surface or physical-interior boundary inside the
+    // tile) every boundary predicate is the constant true/false.
+    auto stencil_pass = [&](auto interior_tag) {
+      constexpr bool IN = decltype(interior_tag)::value;
+      const bool ok0_ = IN || ok0, ok1_ = IN || ok1, u0_ = IN || u0, u1_ = IN || u1;
+      const bool r0_ = IN || r0, r1_ = IN || r1, s0_ = IN || s0, s1_ = IN || s1;
+      if (live && ok0_) {
+        float2 q[CPT + 3];  // vx at columns cb-2 .. cb+CPT
+  #pragma unroll
+        for (int k = 0; k < CPT + 3; ++k) q[k] = VX[(CPT * warp + k) * 32 + lane];
+  #pragma unroll
+        for (int j = 0; j < CPT; ++j) {
+          const int cc = CPT * warp + j;
+          const int c = id.c0 + cc;
+          if (!IN && c >= n2e) continue;
+          const int k = i1 + ld * c;
+          const float* vzc = VZ + cc * (TR + 2 * HR) + 2 * lane;  // row i1-4
+          const float2 zm = *reinterpret_cast<const float2*>(vzc + 2);
+          const float2 z = *reinterpret_cast<const float2*>(vzc + 4);
+          const float zp2 = vzc[6];
+          const int i2p = c - npml;
+          const bool cint = IN || (i2p >= 0 && i2p < g.n2);
+          if (MODE == FM_STAGE_A && it >= 2 && cint && (r0_ || r1_)) {
+            const int ho = h1 + n1h * i2p;
+            const uint64_t pol = l2_evict_first();
+            H::put2(hvs, (int)nih + ho, q[j + 2].x, q[j + 2].y, inv_vx, r0_, r1_, pol);
+            H::put2(hvs, 2 * (int)nih + ho, z.x, z.y, inv_vz, r0_, r1_, pol);
           }
-          if (u1) {
-            const float der2 = dminus(q[j].y, q[j + 1].y, q[j + 2].y, q[j + 3].y);
-            const float der1 = dminus(zm.y, z.x, z.y, zp2);
-            const float kd = fmul(dtdx, kv.y);
-            const float ax = fmul(d2a[j], px_.y), bx = fmul(fmul(kd, d2a1[j]), der2);
-            const float az = fmul(d1a.y, pz_.y), bz = fmul(fmul(kd, d1a1.y), der1);
-            px_.y = fwd ? fadd(ax, bx) : fsub(ax, bx);
-            pz_.y = fwd ? fadd(az, bz) : fsub(az, bz);
+          if (flush) continue;
+          float2 px_ = PX[cc * 32 + lane], pz_ = PZ[cc * 32 + lane];
+          const float2 kv = KA[cc * 32 + lane];
+          if (IN || (c >= 2 && c < hi2)) {
+            const bool fwd = (MODE != FM_STAGE_A);
+            if (u0_) {
+              const float der2 = dminus(q[j].x, q[j + 1].x, q[j + 2].x, q[j + 3].x);
+              const float der1 = dminus(zm.x, zm.y, z.x, z.y);
+              const float kd = fmul(dtdx, kv.x);
+              const float ax = fmul(d2a[j], px_.x), bx = fmul(fmul(kd, d2a1[j]), der2);
+              const float az = fmul(d1a.x, pz_.x), bz = fmul(fmul(kd, d1a1.x), der1);
+              px_.x = fwd ? fadd(ax, bx) : fsub(ax, bx);
+              pz_.x = fwd ? fadd(az, bz) : fsub(az, bz);
+            }
+            if (u1_) {
+              const float der2 = dminus(q[j].y, q[j + 1].y, q[j + 2].y, q[j + 3].y);
+              const float der1 = dminus(zm.y, z.x, z.y, zp2);
+              const float kd = fmul(dtdx, kv.y);
+              const float ax = fmul(d2a[j], px_.y), bx = fmul(fmul(kd, d2a1[j]), der2);
+              const float az = fmul(d1a.y, pz_.y), bz = fmul(fmul(kd, d1a1.y), der1);
+              px_.y = fwd ? fadd(ax, bx) : fsub(ax, bx);
+              pz_.y = fwd ? fadd(az, bz) : fsub(az, bz);
+            }
           }
-        }
-        if (MODE == FM_STAGE_A && ((park >> j) & 1u)) {
-          // receiver band: park the post-stencil pair in the stage buffer for
-          // the band pass after this loop
-          *reinterpret_cast<float2*>(sd.pz + k) = pz_;
-          reinterpret_cast<float2*>(st + kPVX + kPVZ)[cc * 32 + lane] = px_;
-          reinterpret_cast<float2*>(st + kPVX + kPVZ + kPF)[cc * 32 + lane] = pz_;
-          continue;
-        }
-        if (i1 + 1 >= clo[j] && i1 <= chi[j]) {  // forward source
-          const int base = __ldg(sd.inj.col_base + c) - clo[j];
-          const int sg = MODE == FM_FWD ? +1 : -1;
-          if (amp_smem) {
-            if (i1 >= clo[j]) px_.x = inject_at(sd.inj, px_.x, base + i1, dt, kv.x, amp_s, sg);
-            if (ok1 && i1 + 1 <= chi[j])
-              px_.y = inject_at(sd.inj, px_.y, base + i1 + 1, dt, kv.y, amp_s, sg);
-          } else {
-            if (i1 >= clo[j])
-              px_.x = inject_at_global(sd.inj, px_.x, base + i1, dt, kv.x, sd.amp + (it - 1),
-                                       sd.amp_stride, sg);
-            if (ok1 && i1 + 1 <= chi[j])
-              px_.y = inject_at_global(sd.inj, px_.y, base + i1 + 1, dt, kv.y, sd.amp + (it - 1),
-                                       sd.amp_stride, sg);
+          if (MODE == FM_STAGE_A && ((park >> j) & 1u)) {
+            // receiver band: park the post-stencil pair in the stage buffer for
+            // the band pass after this loop
+            *reinterpret_cast<float2*>(sd.pz + k) = pz_;
+            reinterpret_cast<float2*>(st + kPVX + kPVZ)[cc * 32 + lane] = px_;
+            reinterpret_cast<float2*>(st + kPVX + kPVZ + kPF)[cc * 32 + lane] = pz_;
+            continue;
           }
-        }
-        if (kB && i2p >= slo && i2p < shi2 && (s0 || s1)) {
-          const float2 hv = hist_box_read<FP16>(st + kPStage, cc, lane);
-          if (s0) px_.x = fadd(px_.x, fmul(fmul(mdt, hv.x * sc_p), kv.x));
-          if (s1) px_.y = fadd(px_.y, fmul(fmul(mdt, hv.y * sc_p), kv.y));
-        }
-        float2 pv;
-        pv.x = i1 < fsrows ? 0.f : fadd(px_.x, pz_.x);
-        pv.y = i1 + 1 < fsrows ? 0.f : fadd(px_.y, pz_.y);
-        *reinterpret_cast<float2*>(sd.px + k) = px_;
-        *reinterpret_cast<float2*>(sd.pz + k) = pz_;
-        *reinterpret_cast<float2*>(sd.p + k) = pv;
-        if (cint) {
-          if (MODE == FM_STAGE_A) {
-            if (r0) lmax = max(lmax, abs_bits(pv.x));
-            if (r1) lmax = max(lmax, abs_bits(pv.y));
-          }
-          if ((MODE == FM_FWD || MODE == FM_STAGE_B_ES) && sd.wf && sd.type_rec == 0) {
-            float* w = sd.wf + (size_t)(it - 1) * g.int_elems() + (size_t)g.n1 * i2p;
-            const int i1p = i1 - npml;
-            if (MODE == FM_FWD) {
-              if (r0) w[i1p] = pv.x;
-              if (r1) w[i1p + 1] = pv.y;
+          if (i1 + 1 >= clo[j] && i1 <= chi[j]) {  // forward source
+            const int base = __ldg(sd.inj.col_base + c) - clo[j];
+            const int sg = MODE == FM_FWD ? +1 : -1;
+            if (amp_smem) {
+              if (i1 >= clo[j]) px_.x = inject_at(sd.inj, px_.x, base + i1, dt, kv.x, amp_s, sg);
+              if (ok1_ && i1 + 1 <= chi[j])
+                px_.y = inject_at(sd.inj, px_.y, base + i1 + 1, dt, kv.y, amp_s, sg);
             } else {
-              if (r0) w[i1p] = fadd(w[i1p], pv.x);
-              if (r1) w[i1p + 1] = fadd(w[i1p + 1], pv.y);
+              if (i1 >= clo[j])
+                px_.x = inject_at_global(sd.inj, px_.x, base + i1, dt, kv.x, sd.amp + (it - 1),
+                                         sd.amp_stride, sg);
+              if (ok1_ && i1 + 1 <= chi[j])
+                px_.y = inject_at_global(sd.inj, px_.y, base + i1 + 1, dt, kv.y, sd.amp + (it - 1),
+                                         sd.amp_stride, sg);
+            }
+          }
+          if (kB && (IN || (i2p >= slo && i2p < shi2)) && (s0_ || s1_)) {
+            const float2 hv = hist_box_read<FP16>(st + kPStage, cc, lane);
+            if (s0_) px_.x = fadd(px_.x, fmul(fmul(mdt, hv.x * sc_p), kv.x));
+            if (s1_) px_.y = fadd(px_.y, fmul(fmul(mdt, hv.y * sc_p), kv.y));
+          }
+          float2 pv;
+          pv.x = (!IN && i1 < fsrows) ? 0.f : fadd(px_.x, pz_.x);
+          pv.y = (!IN && i1 + 1 < fsrows) ? 0.f : fadd(px_.y, pz_.y);
+          *reinterpret_cast<float2*>(sd.px + k) = px_;
+          *reinterpret_cast<float2*>(sd.pz + k) = pz_;
+          *reinterpret_cast<float2*>(sd.p + k) = pv;
+          if (cint) {
+            if (MODE == FM_STAGE_A) {
+              if (r0_) lmax = max(lmax, abs_bits(pv.x));
+              if (r1_) lmax = max(lmax, abs_bits(pv.y));
+            }
+            if ((MODE == FM_FWD || MODE == FM_STAGE_B_ES) && sd.wf && sd.type_rec == 0) {
+              float* w = sd.wf + (size_t)(it - 1) * g.int_elems() + (size_t)g.n1 * i2p;
+              const int i1p = i1 - npml;
+              if (MODE == FM_FWD) {
+                if (r0_) w[i1p] = pv.x;
+                if (r1_) w[i1p + 1] = pv.y;
+              } else {
+                if (r0_) w[i1p] = fadd(w[i1p], pv.x);
+                if (r1_) w[i1p + 1] = fadd(w[i1p + 1], pv.y);
+              }
             }
           }
         }
       }
-    }
+    };
+    if (tile_interior(g, id, MODE, slo, shi1, shi2))
+      stencil_pass(std::true_type{});
+    else
+      stencil_pass(std::false_type{});
     if (MODE == FM_STAGE_A) {
       // Receiver band of this tile: each warp finishes the parked rows of its
       // own columns, one lane per row.  The row pointers of all its columns
@@ -828,86 +857,97 @@ __global__ void __launch_bounds__(kThreadsT, 2)
     const float2* P2 = reinterpret_cast<const float2*>(st);
     const float2* VX = reinterpret_cast<const float2*>(st + kVP);
     const float2* VZ = VX + TR * TC / 2;
-    if (live && ok0) {
-      float2 a[CPT + 3];  // p rows (i1, i1+1) at columns cb-1 .. cb+CPT+1
-#pragma unroll
-      for (int k = 0; k < CPT + 3; ++k) a[k] = P2[(CPT * warp + k) * ((TR + 2 * HR) / 2) + 2 + lane];
-      const bool dst_x = fs && i1 == npml - 1;
-      const bool skip_y = fs && i1 + 1 == npml - 1;
-      const bool src_x = fs && i1 == npml;
-#pragma unroll
-      for (int j = 0; j < CPT; ++j) {
-        const int cc = CPT * warp + j;
-        const int c = id.c0 + cc;
-        if (c >= n2e) continue;
-        const int k = i1 + ld * c;
-        const float* pcol = P + (cc + 1) * (TR + 2 * HR) + 2 * lane;  // own column, row i1-4
-        const float pm1 = pcol[3];
-        const float2 pc = a[j + 1];
-        const float2 pp = *reinterpret_cast<const float2*>(pcol + 6);
-        const int i2p = c - npml;
-        const bool cint = i2p >= 0 && i2p < g.n2;
-        float2 vx_ = VX[cc * 32 + lane], vz_ = VZ[cc * 32 + lane];
-        if (c >= 2 && c < hi2) {
-          const bool fwd = (MODE != FM_STAGE_A);
-          if (u0) {
-            const float der2 = dplus(a[j].x, pc.x, a[j + 2].x, a[j + 3].x);
-            const float der1 = dplus(pm1, pc.x, pc.y, pp.x);
-            const float ax = fmul(d2b[j], vx_.x), bx = fmul(bw2[j], der2);
-            const float az = fmul(d1b.x, vz_.x), bz = fmul(bw1.x, der1);
-            vx_.x = fwd ? fadd(ax, bx) : fsub(ax, bx);
-            vz_.x = fwd ? fadd(az, bz) : fsub(az, bz);
+    // The stencil pass, compiled twice (interior tiles: every boundary
+    // predicate constant, as in the pressure kernel).
+    auto stencil_pass = [&](auto interior_tag) {
+      constexpr bool IN = decltype(interior_tag)::value;
+      const bool ok0_ = IN || ok0, ok1_ = IN || ok1, u0_ = IN || u0, u1_ = IN || u1;
+      const bool r0_ = IN || r0, r1_ = IN || r1;
+      if (live && ok0_) {
+        float2 a[CPT + 3];  // p rows (i1, i1+1) at columns cb-1 .. cb+CPT+1
+  #pragma unroll
+        for (int k = 0; k < CPT + 3; ++k) a[k] = P2[(CPT * warp + k) * ((TR + 2 * HR) / 2) + 2 + lane];
+        const bool dst_x = !IN && fs && i1 == npml - 1;
+        const bool skip_y = !IN && fs && i1 + 1 == npml - 1;
+        const bool src_x = !IN && fs && i1 == npml;
+  #pragma unroll
+        for (int j = 0; j < CPT; ++j) {
+          const int cc = CPT * warp + j;
+          const int c = id.c0 + cc;
+          if (!IN && c >= n2e) continue;
+          const int k = i1 + ld * c;
+          const float* pcol = P + (cc + 1) * (TR + 2 * HR) + 2 * lane;  // own column, row i1-4
+          const float pm1 = pcol[3];
+          const float2 pc = a[j + 1];
+          const float2 pp = *reinterpret_cast<const float2*>(pcol + 6);
+          const int i2p = c - npml;
+          const bool cint = IN || (i2p >= 0 && i2p < g.n2);
+          float2 vx_ = VX[cc * 32 + lane], vz_ = VZ[cc * 32 + lane];
+          if (IN || (c >= 2 && c < hi2)) {
+            const bool fwd = (MODE != FM_STAGE_A);
+            if (u0_) {
+              const float der2 = dplus(a[j].x, pc.x, a[j + 2].x, a[j + 3].x);
+              const float der1 = dplus(pm1, pc.x, pc.y, pp.x);
+              const float ax = fmul(d2b[j], vx_.x), bx = fmul(bw2[j], der2);
+              const float az = fmul(d1b.x, vz_.x), bz = fmul(bw1.x, der1);
+              vx_.x = fwd ? fadd(ax, bx) : fsub(ax, bx);
+              vz_.x = fwd ? fadd(az, bz) : fsub(az, bz);
+            }
+            if (u1_) {
+              const float der2 = dplus(a[j].y, pc.y, a[j + 2].y, a[j + 3].y);
+              const float der1 = dplus(pc.x, pc.y, pp.x, pp.y);
+              const float ax = fmul(d2b[j], vx_.y), bx = fmul(bw2[j], der2);
+              const float az = fmul(d1b.y, vz_.y), bz = fmul(bw1.y, der1);
+              vx_.y = fwd ? fadd(ax, bx) : fsub(ax, bx);
+              vz_.y = fwd ? fadd(az, bz) : fsub(az, bz);
+            }
           }
-          if (u1) {
-            const float der2 = dplus(a[j].y, pc.y, a[j + 2].y, a[j + 3].y);
-            const float der1 = dplus(pc.x, pc.y, pp.x, pp.y);
-            const float ax = fmul(d2b[j], vx_.y), bx = fmul(bw2[j], der2);
-            const float az = fmul(d1b.y, vz_.y), bz = fmul(bw1.y, der1);
-            vx_.y = fwd ? fadd(ax, bx) : fsub(ax, bx);
-            vz_.y = fwd ? fadd(az, bz) : fsub(az, bz);
+          if (kB && cint && (r0_ || r1_)) {
+            const float2 hx = hist_box_read<FP16>(st + kVStage, cc, lane);
+            const float2 hz = hist_box_read<FP16>(st + kVStage + hist_box(FP16), cc, lane);
+            if (r0_) {
+              vx_.x = fadd(vx_.x, fmul(fmul(mdt, hx.x * sc_vx), 1.0f));
+              vz_.x = fadd(vz_.x, fmul(fmul(mdt, hz.x * sc_vz), 1.0f));
+            }
+            if (r1_) {
+              vx_.y = fadd(vx_.y, fmul(fmul(mdt, hx.y * sc_vx), 1.0f));
+              vz_.y = fadd(vz_.y, fmul(fmul(mdt, hz.y * sc_vz), 1.0f));
+            }
           }
-        }
-        if (kB && cint && (r0 || r1)) {
-          const float2 hx = hist_box_read<FP16>(st + kVStage, cc, lane);
-          const float2 hz = hist_box_read<FP16>(st + kVStage + hist_box(FP16), cc, lane);
-          if (r0) {
-            vx_.x = fadd(vx_.x, fmul(fmul(mdt, hx.x * sc_vx), 1.0f));
-            vz_.x = fadd(vz_.x, fmul(fmul(mdt, hz.x * sc_vz), 1.0f));
+          if (i1 + 1 >= clo[j] && i1 <= chi[j]) {  // vz source (type_src = 1)
+            const int base = __ldg(sd.inj.col_base + c) - clo[j];
+            if (i1 >= clo[j])
+              vz_.x = inject_at_global(sd.inj, vz_.x, base + i1, dt, 1.0f, sd.amp + (it - 1),
+                                       sd.amp_stride, +1);
+            if (ok1_ && i1 + 1 <= chi[j])
+              vz_.y = inject_at_global(sd.inj, vz_.y, base + i1 + 1, dt, 1.0f, sd.amp + (it - 1),
+                                       sd.amp_stride, +1);
           }
-          if (r1) {
-            vx_.y = fadd(vx_.y, fmul(fmul(mdt, hx.y * sc_vx), 1.0f));
-            vz_.y = fadd(vz_.y, fmul(fmul(mdt, hz.y * sc_vz), 1.0f));
-          }
-        }
-        if (i1 + 1 >= clo[j] && i1 <= chi[j]) {  // vz source (type_src = 1)
-          const int base = __ldg(sd.inj.col_base + c) - clo[j];
-          if (i1 >= clo[j])
-            vz_.x = inject_at_global(sd.inj, vz_.x, base + i1, dt, 1.0f, sd.amp + (it - 1),
-                                     sd.amp_stride, +1);
-          if (ok1 && i1 + 1 <= chi[j])
-            vz_.y = inject_at_global(sd.inj, vz_.y, base + i1 + 1, dt, 1.0f, sd.amp + (it - 1),
-                                     sd.amp_stride, +1);
-        }
-        if (dst_x) vz_.x = vz_.y;
-        *reinterpret_cast<float2*>(sd.vx + k) = vx_;
-        if (skip_y)
-          sd.vz[k] = vz_.x;
-        else
-          *reinterpret_cast<float2*>(sd.vz + k) = vz_;
-        if (src_x) sd.vz[k - 1] = vz_.x;
-        if (MODE == FM_STAGE_A && cint && (r0 || r1)) {
-          Hist<FP16>::put2(hps, h1 + n1h * i2p, pc.x, pc.y, inv_p, r0, r1, l2_evict_first());
-          if (r0) {
-            lmx = max(lmx, abs_bits(vx_.x));
-            lmz = max(lmz, abs_bits(vz_.x));
-          }
-          if (r1) {
-            lmx = max(lmx, abs_bits(vx_.y));
-            lmz = max(lmz, abs_bits(vz_.y));
+          if (dst_x) vz_.x = vz_.y;
+          *reinterpret_cast<float2*>(sd.vx + k) = vx_;
+          if (skip_y)
+            sd.vz[k] = vz_.x;
+          else
+            *reinterpret_cast<float2*>(sd.vz + k) = vz_;
+          if (src_x) sd.vz[k - 1] = vz_.x;
+          if (MODE == FM_STAGE_A && cint && (r0_ || r1_)) {
+            Hist<FP16>::put2(hps, h1 + n1h * i2p, pc.x, pc.y, inv_p, r0_, r1_, l2_evict_first());
+            if (r0_) {
+              lmx = max(lmx, abs_bits(vx_.x));
+              lmz = max(lmz, abs_bits(vz_.x));
+            }
+            if (r1_) {
+              lmx = max(lmx, abs_bits(vx_.y));
+              lmz = max(lmz, abs_bits(vz_.y));
+            }
           }
         }
       }
-    }
+    };
+    if (tile_interior(g, id, MODE, 0, g.n1, g.n2))
+      stencil_pass(std::true_type{});
+    else
+      stencil_pass(std::false_type{});
     __syncthreads();
     stage ^= 1;
   }
