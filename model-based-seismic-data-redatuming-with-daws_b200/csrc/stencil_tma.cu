@@ -464,6 +464,9 @@ __global__ void __launch_bounds__(kThreadsT, 2)
     const bool s0 = r0 && i1 - npml >= slo && i1 - npml < shi1;
     const bool s1 = r1 && i1 + 1 - npml >= slo && i1 + 1 - npml < shi1;
     const int cb = id.c0 + CPT * warp;
+    // Interior tiles lie inside the physical region, where every sponge factor
+    // is exactly 1 (x * 1 == x), so they load no profiles.
+    const bool interior = tile_interior(g, id, MODE, slo, shi1, shi2);
     // ---- global prefetch before waiting for the tile
     float2 d1a = make_float2(0.f, 0.f), d1a1 = make_float2(0.f, 0.f);
     float d2a[CPT], d2a1[CPT];
@@ -471,7 +474,7 @@ __global__ void __launch_bounds__(kThreadsT, 2)
     // Stage A: the receiver band of column cb + lane is held by lane < CPT
     // (first row, last row, dense-row base) and shuffled out when needed.
     int bl = 0x7fffffff, bh = -1, bb = 0;
-    if (live && !flush) {
+    if (live && !flush && !interior) {
       if (ok1) {
         d1a = ldg2(m.d1a + i1);
         d1a1 = ldg2(m.d1a1 + i1);
@@ -484,8 +487,8 @@ __global__ void __launch_bounds__(kThreadsT, 2)
     for (int j = 0; j < CPT; ++j) {
       const int c = cb + j;
       const bool cok = live && !flush && c < n2e;
-      d2a[j] = cok ? __ldg(m.d2a + c) : 0.f;
-      d2a1[j] = cok ? __ldg(m.d2a1 + c) : 0.f;
+      d2a[j] = cok && !interior ? __ldg(m.d2a + c) : 0.f;
+      d2a1[j] = cok && !interior ? __ldg(m.d2a1 + c) : 0.f;
       clo[j] = (MODE != FM_STAGE_A && cok && do_inj) ? __ldg(sd.inj.col_lo + c) : 0x7fffffff;
       chi[j] = (MODE != FM_STAGE_A && cok && do_inj) ? __ldg(sd.inj.col_hi + c) : -1;
     }
@@ -548,8 +551,10 @@ __global__ void __launch_bounds__(kThreadsT, 2)
               const float der2 = dminus(q[j].x, q[j + 1].x, q[j + 2].x, q[j + 3].x);
               const float der1 = dminus(zm.x, zm.y, z.x, z.y);
               const float kd = fmul(dtdx, kv.x);
-              const float ax = fmul(d2a[j], px_.x), bx = fmul(fmul(kd, d2a1[j]), der2);
-              const float az = fmul(d1a.x, pz_.x), bz = fmul(fmul(kd, d1a1.x), der1);
+              const float ax = IN ? px_.x : fmul(d2a[j], px_.x);
+              const float bx = IN ? fmul(kd, der2) : fmul(fmul(kd, d2a1[j]), der2);
+              const float az = IN ? pz_.x : fmul(d1a.x, pz_.x);
+              const float bz = IN ? fmul(kd, der1) : fmul(fmul(kd, d1a1.x), der1);
               px_.x = fwd ? fadd(ax, bx) : fsub(ax, bx);
               pz_.x = fwd ? fadd(az, bz) : fsub(az, bz);
             }
@@ -557,8 +562,10 @@ __global__ void __launch_bounds__(kThreadsT, 2)
               const float der2 = dminus(q[j].y, q[j + 1].y, q[j + 2].y, q[j + 3].y);
               const float der1 = dminus(zm.y, z.x, z.y, zp2);
               const float kd = fmul(dtdx, kv.y);
-              const float ax = fmul(d2a[j], px_.y), bx = fmul(fmul(kd, d2a1[j]), der2);
-              const float az = fmul(d1a.y, pz_.y), bz = fmul(fmul(kd, d1a1.y), der1);
+              const float ax = IN ? px_.y : fmul(d2a[j], px_.y);
+              const float bx = IN ? fmul(kd, der2) : fmul(fmul(kd, d2a1[j]), der2);
+              const float az = IN ? pz_.y : fmul(d1a.y, pz_.y);
+              const float bz = IN ? fmul(kd, der1) : fmul(fmul(kd, d1a1.y), der1);
               px_.y = fwd ? fadd(ax, bx) : fsub(ax, bx);
               pz_.y = fwd ? fadd(az, bz) : fsub(az, bz);
             }
@@ -618,7 +625,7 @@ __global__ void __launch_bounds__(kThreadsT, 2)
         }
       }
     };
-    if (tile_interior(g, id, MODE, slo, shi1, shi2))
+    if (interior)
       stencil_pass(std::true_type{});
     else
       stencil_pass(std::false_type{});
@@ -772,6 +779,7 @@ __global__ void __launch_bounds__(kThreadsT, 2)
   const int n1h = L.n1h;
   const size_t nih = (size_t)n1h * g.n2;
   const float dt = g.dt, mdt = fmul(-1.0f, dt);
+  const float dtdx_v = fmul(g.dtdx, 1.0f);  // bw1 = bw2 in the physical interior
   const bool fs = g.ofs == 1;
   int cur = -1;
   ShotDevice sd;
@@ -829,8 +837,10 @@ __global__ void __launch_bounds__(kThreadsT, 2)
     const bool r1 = ok1 && i1 + 1 >= npml && i1 + 1 < npml + g.n1;
     const int h1 = i1 - hbase;
     const int cb = id.c0 + CPT * warp;
+    // interior tiles: sponge factors exactly 1, bw1 = bw2 = dtdx
+    const bool interior = tile_interior(g, id, MODE, 0, g.n1, g.n2);
     float2 d1b = make_float2(0.f, 0.f), bw1 = make_float2(0.f, 0.f);
-    if (live) {
+    if (live && !interior) {
       if (ok1) {
         d1b = ldg2(m.d1b + i1);
         bw1 = ldg2(m.bw1 + i1);
@@ -845,8 +855,8 @@ __global__ void __launch_bounds__(kThreadsT, 2)
     for (int j = 0; j < CPT; ++j) {
       const int c = cb + j;
       const bool cok = live && c < n2e;
-      d2b[j] = cok ? __ldg(m.d2b + c) : 0.f;
-      bw2[j] = cok ? __ldg(m.bw2 + c) : 0.f;
+      d2b[j] = cok && !interior ? __ldg(m.d2b + c) : 0.f;
+      bw2[j] = cok && !interior ? __ldg(m.bw2 + c) : 0.f;
       clo[j] = (cok && do_inj) ? __ldg(sd.inj.col_lo + c) : 0x7fffffff;
       chi[j] = (cok && do_inj) ? __ldg(sd.inj.col_hi + c) : -1;
     }
@@ -888,16 +898,20 @@ __global__ void __launch_bounds__(kThreadsT, 2)
             if (u0_) {
               const float der2 = dplus(a[j].x, pc.x, a[j + 2].x, a[j + 3].x);
               const float der1 = dplus(pm1, pc.x, pc.y, pp.x);
-              const float ax = fmul(d2b[j], vx_.x), bx = fmul(bw2[j], der2);
-              const float az = fmul(d1b.x, vz_.x), bz = fmul(bw1.x, der1);
+              const float ax = IN ? vx_.x : fmul(d2b[j], vx_.x);
+              const float bx = fmul(IN ? dtdx_v : bw2[j], der2);
+              const float az = IN ? vz_.x : fmul(d1b.x, vz_.x);
+              const float bz = fmul(IN ? dtdx_v : bw1.x, der1);
               vx_.x = fwd ? fadd(ax, bx) : fsub(ax, bx);
               vz_.x = fwd ? fadd(az, bz) : fsub(az, bz);
             }
             if (u1_) {
               const float der2 = dplus(a[j].y, pc.y, a[j + 2].y, a[j + 3].y);
               const float der1 = dplus(pc.x, pc.y, pp.x, pp.y);
-              const float ax = fmul(d2b[j], vx_.y), bx = fmul(bw2[j], der2);
-              const float az = fmul(d1b.y, vz_.y), bz = fmul(bw1.y, der1);
+              const float ax = IN ? vx_.y : fmul(d2b[j], vx_.y);
+              const float bx = fmul(IN ? dtdx_v : bw2[j], der2);
+              const float az = IN ? vz_.y : fmul(d1b.y, vz_.y);
+              const float bz = fmul(IN ? dtdx_v : bw1.y, der1);
               vx_.y = fwd ? fadd(ax, bx) : fsub(ax, bx);
               vz_.y = fwd ? fadd(az, bz) : fsub(az, bz);
             }
@@ -944,7 +958,7 @@ __global__ void __launch_bounds__(kThreadsT, 2)
         }
       }
     };
-    if (tile_interior(g, id, MODE, 0, g.n1, g.n2))
+    if (interior)
       stencil_pass(std::true_type{});
     else
       stencil_pass(std::false_type{});
