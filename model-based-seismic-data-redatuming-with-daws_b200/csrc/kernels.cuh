@@ -40,16 +40,30 @@ __device__ __forceinline__ float warp_gather_ordered(float* prod, const int* ix1
   const int r1a = max(1 - ix1, -kRad), r1b = min(hi1 - ix1, kRad);
   const int r2a = max(1 - ix2, -kRad), r2b = min(hi2 - ix2, kRad);
   const float* tile = tiles + (size_t)s * kTile;
-  for (int t = lane; t < 444; t += 32) {
-    float v = 0.f;
-    if (t < kTile) {
-      const int a = t / kTap - kRad, b = t % kTap - kRad;
-      if (a >= r1a && a <= r1b && b >= r2a && b <= r2b)
-        v = fmul(__ldg(tile + (a + kRad) + kTap * (b + kRad)),
-                 origin[(ix1 + a - 1) + (size_t)ld * (ix2 + b - 1)]);
+  // Lane l owns taps t = l + 32 k (k < 14); all 28 loads are issued before
+  // the products, so their latencies overlap.  Tap t = (a+10)*21 + (b+10):
+  // stepping t by 32 = 21 + 11 steps b by 11 and a by 1 (or 2 on wrap).
+  constexpr int kSteps = (444 + 31) / 32;
+  float tv[kSteps], pv[kSteps];
+  {
+    int a = lane / kTap - kRad, b = lane % kTap - kRad;
+#pragma unroll
+    for (int k = 0; k < kSteps; ++k) {
+      const int t = lane + 32 * k;
+      const bool in = t < kTile && a >= r1a && a <= r1b && b >= r2a && b <= r2b;
+      tv[k] = in ? __ldg(tile + (a + kRad) + kTap * (b + kRad)) : 0.f;
+      pv[k] = in ? origin[(ix1 + a - 1) + (size_t)ld * (ix2 + b - 1)] : 0.f;
+      b += 32 - kTap;
+      a += 1;
+      if (b > kRad) {
+        b -= kTap;
+        a += 1;
+      }
     }
-    prod[t] = v;
   }
+#pragma unroll
+  for (int k = 0; k < kSteps; ++k)
+    if (lane + 32 * k < 444) prod[lane + 32 * k] = fmul(tv[k], pv[k]);  // +0 outside the support
   __syncwarp();
   float acc = 0.f;
   if (lane == 0) {
