@@ -18,7 +18,7 @@
 //
 // Stage A injects the residual at every receiver (441 taps each, summed per
 // grid point in station order).  Tiles crossing that band park their
-// post-stencil pressure pairs in the stage buffer; after a CTA barrier each
+// post-stencil pressure pairs in the stage buffer; after a warp barrier each
 // warp finishes the band rows of its own columns with one lane per row,
 // issuing the row pointers and the tap entries of several points as batches
 // so that the dependent loads overlap.
@@ -635,8 +635,11 @@ __global__ void __launch_bounds__(kThreadsT, 2)
       // are loaded first, then each point's entries as one batch; the sum
       // keeps the station order.
       const int rlast = min(id.r0 + TR, n1e) - 1;
+      // A warp only reads row pairs parked by its own lanes (its own
+      // columns), so a warp vote and a warp barrier order the pass.
       const bool wb = lane < CPT && bl <= rlast && bh >= id.r0;
-      if (__syncthreads_or(wb)) {  // CTA-uniform; also orders the parked pairs
+      if (__any_sync(kAll, wb)) {  // warp-uniform
+        __syncwarp();
         const float* PXf = reinterpret_cast<const float*>(st + kPVX + kPVZ);
         const float* PZf = PXf + TR * TC;
         const float* KAf = PZf + TR * TC;
