@@ -224,6 +224,12 @@ void daw_reset_timing(daw_handle* h);
 void daw_hicks_tile(int32_t ialpha1, int32_t ialpha2, int32_t nalpha_frees, float* tile);
 void daw_hicks_locate(float z, float x, float hgrid, int32_t ofs, int32_t* out5);
 
+/* Diagnostic (no counterpart in the reference): runs one device-side
+ * bounded wait that nothing completes, with a ~0.5 ms budget, and returns
+ * what the library reports when a wait runs out -- DAW_ERR_TIMEOUT when the
+ * failure path works.  No GPU fault is involved; the handle stays usable. */
+int daw_selftest_wait_timeout(daw_handle* h);
+
 /* Library version string. */
 const char* daw_version(void);
 

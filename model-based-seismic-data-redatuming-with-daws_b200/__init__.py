@@ -122,6 +122,7 @@ def _declare(L):
     L.daw_reset_timing.argtypes = [vp]
     L.daw_reset_timing.restype = None
     L.daw_version.restype = C.c_char_p
+    L.daw_selftest_wait_timeout.argtypes = [vp]
     L.daw_hicks_tile.argtypes = [i32, i32, i32, fp]
     L.daw_hicks_tile.restype = None
     L.daw_hicks_locate.argtypes = [f32, f32, f32, i32, ip]

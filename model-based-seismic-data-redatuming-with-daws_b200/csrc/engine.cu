@@ -1621,6 +1621,17 @@ int daw_shots(daw_handle* h, int32_t n, const daw_shot_desc* descs, daw_shot_out
   });
 }
 
+int daw_selftest_wait_timeout(daw_handle* h) {
+  if (!h) return DAW_ERR_ARG;
+  const int rc = guarded(h, [&] {
+    tma_wait_selftest(h->d_err, 1LL << 20, h->st);  // ~0.5 ms at the SM clock
+    check_launch("wait self-test");
+    sync(h);
+    check_device_error(h);
+  });
+  return rc;
+}
+
 int daw_get_timing(const daw_handle* h, daw_timing* t) {
   if (!h || !t) return DAW_ERR_ARG;
   *t = h->tim;

@@ -79,6 +79,9 @@ struct FusedLaunch {
 // TMA kernels (stencil_tma.cu)
 int tma_tiles(const Grid& g);
 void tma_prepare(int* persist_p, int* persist_v);
+// One bounded mbarrier wait that nothing completes: raises kErrTimeout in
+// *err after `budget` cycles.
+void tma_wait_selftest(unsigned* err, long long budget, cudaStream_t st);
 void tma_p_step(const Grid& g, const ModelDev& m, const FusedLaunch& L, int mode, int it,
                 cudaStream_t st);
 void tma_v_step(const Grid& g, const ModelDev& m, const FusedLaunch& L, int mode, int it,

@@ -92,13 +92,15 @@ __device__ __forceinline__ bool bar_try(uint64_t* b, uint32_t parity) {
       : "memory");
   return ok != 0;
 }
-// Bounded wait: ~2^31 cycles, then the error flag is raised and the caller
-// proceeds (results of that launch are then invalid; the host reports it).
-__device__ __forceinline__ void bar_wait(uint64_t* b, uint32_t parity, unsigned* err) {
+// Bounded wait: `budget` cycles (~1 s by default), then the error flag is
+// raised and the caller proceeds (results of that launch are then invalid;
+// the host reports it).
+__device__ __forceinline__ void bar_wait(uint64_t* b, uint32_t parity, unsigned* err,
+                                         long long budget = 1LL << 31) {
   if (bar_try(b, parity)) return;
   const long long t0 = clock64();
   while (!bar_try(b, parity)) {
-    if (clock64() - t0 > (1LL << 31)) {
+    if (clock64() - t0 > budget) {
       atomicOr(err, kErrTimeout);
       return;
     }
@@ -1037,7 +1039,24 @@ void prep_mode(int* pp, int* pv) {
   *pv = std::min(*pv, occupancy(k_tma_v<MODE, FP16>, v_smem(MODE, FP16)));
 }
 
+// Self-test of the failure path of the bounded waits: thread 0 waits on an
+// mbarrier that no copy and no thread will complete, with a short budget; the
+// wait gives up, raises kErrTimeout and returns (no copy is in flight).
+__global__ void k_wait_selftest(unsigned* err, long long budget) {
+  __shared__ __align__(8) uint64_t b;
+  if (threadIdx.x == 0) {
+    bar_init(&b);
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) bar_wait(&b, 0, err, budget);
+}
+
 }  // namespace
+
+void tma_wait_selftest(unsigned* err, long long budget, cudaStream_t st) {
+  k_wait_selftest<<<1, 32, 0, st>>>(err, budget);
+}
 
 int tma_tiles(const Grid& g) { return ((g.n1e + TR - 1) / TR) * ((g.n2e + TC - 1) / TC); }
 

@@ -291,3 +291,15 @@ def test_non_finite_history_is_reported(pkg, case, opt):
         res[7, 3] = 1.0
         g = h.submodeling_adjoint_esource_data(res, case["rec"])
         assert np.isfinite(g).all() and np.abs(g).max() > 0
+
+
+def test_bounded_wait_reports_timeout(pkg, case):
+    """The failure path of the device-side bounded waits: a wait that nothing
+    completes gives up after its budget and is reported as DAW_ERR_TIMEOUT;
+    no GPU fault is involved and the handle keeps working afterwards."""
+    w = case["w"]
+    with handle(pkg, case, preset="mixed") as h:
+        assert pkg.lib().daw_selftest_wait_timeout(h._h) == -4
+        assert "bounded device wait" in pkg.lib().daw_last_error(h._h).decode()
+        sis, _ = h.submodeling(case["s"], case["src"], case["rec"])
+        assert np.isfinite(sis).all() and np.abs(sis).max() > 0
