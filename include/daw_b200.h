@@ -191,6 +191,15 @@ int daw_shot(daw_handle* h, const daw_shot_desc* desc, daw_shot_out* out);
  * descs[i]. */
 int daw_shots(daw_handle* h, int32_t n, const daw_shot_desc* descs, daw_shot_out* outs);
 
+/* Batched forward modelling, mode 0 (sub_redatum_DAW.f90:55-72: submodeling
+ * of every shot in the true model).  No history is kept, so up to 64 shots
+ * share each launch.  descs[i] supplies s, nt, src_tab, rec_tab, nrec,
+ * type_src, type_rec (other fields ignored); sis[i] receives that shot's
+ * (nt, nrec) receiver data.  For the wavefield output (oio = 1) call
+ * daw_submodeling per shot. */
+int daw_submodeling_shots(daw_handle* h, int32_t n, const daw_shot_desc* descs,
+                          float* const* sis);
+
 /* Device-resident timing support: shots whose inputs were staged once with
  * daw_stage_shots run with no host transfers; results stay on the device
  * until daw_fetch_shots. ms_out (nullable) receives the device time. */

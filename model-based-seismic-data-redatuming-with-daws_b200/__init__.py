@@ -114,6 +114,7 @@ def _declare(L):
                                           C.c_char_p, i32]
     L.daw_shot.argtypes = [vp, C.POINTER(ShotDesc), C.POINTER(ShotOut)]
     L.daw_shots.argtypes = [vp, i32, C.POINTER(ShotDesc), C.POINTER(ShotOut)]
+    L.daw_submodeling_shots.argtypes = [vp, i32, C.POINTER(ShotDesc), C.POINTER(fp)]
     L.daw_stage_shots.argtypes = [vp, i32, C.POINTER(ShotDesc)]
     L.daw_run_staged.argtypes = [vp, fp]
     L.daw_fetch_shots.argtypes = [vp, C.POINTER(ShotOut)]
@@ -244,6 +245,35 @@ class Handle:
                                        type_src, type_rec, _p(ir, C.c_int32), nr,
                                        _p(sis, C.c_float), _p(wf, C.c_float)))
         return sis, wf
+
+    def submodeling_shots(self, shots):
+        """Batched forward modelling (mode 0): `shots` are dicts with s, src,
+        rec and optionally nt, type_src, type_rec; returns each shot's
+        (nt, nrec) receiver data."""
+        n = len(shots)
+        descs = (ShotDesc * n)()
+        outs = (C.POINTER(C.c_float) * n)()
+        keep, results = [], []
+        for i, sh in enumerate(shots):
+            s = _f32(sh["s"])
+            rec = _i32(sh["rec"])
+            nt = int(sh.get("nt", s.shape[0]))
+            sis = np.zeros((nt, rec.shape[0]), np.float32, order="F")
+            keep += [s, rec]
+            results.append(sis)
+            d = descs[i]
+            d.shot = int(sh.get("shot", i + 1))
+            d.nt = nt
+            d.s = _p(s, C.c_float)
+            for k in range(5):
+                d.src_tab[k] = int(sh["src"][k])
+            d.rec_tab = _p(rec, C.c_int32)
+            d.nrec = rec.shape[0]
+            d.type_src = int(sh.get("type_src", 0))
+            d.type_rec = int(sh.get("type_rec", 0))
+            outs[i] = _p(sis, C.c_float)
+        self._ck(lib().daw_submodeling_shots(self._h, n, descs, outs))
+        return results
 
     def submodeling_adjoint_esource_data(self, res, ir, type_rec=0):
         res = _f32(res)

@@ -154,6 +154,64 @@ extern "C" int daw_run_parfile(daw_handle* h, const char* workdir_c, int32_t fir
     b = std::min(b, nsrc);
     float band[4] = {pf.flow, pf.fhig, pf.llow, pf.lhig};
     const size_t nd = (size_t)nt * nrec, ni = (size_t)n1 * n2;
+    // Without wavefield files (oio != 1), modes 0 and 1 run shots in batches
+    // through the batched entry points; the files written are the same.
+    if ((pf.mode == 0 || pf.mode == 1) && pf.oio != 1) {
+      const int chunk = pf.mode == 0 ? 32 : 8;
+      for (int c0 = a; c0 <= b; c0 += chunk) {
+        const int cnt = std::min(b, c0 + chunk - 1) - c0 + 1;
+        std::vector<daw_shot_desc> descs(cnt);
+        std::vector<std::vector<float>> data(cnt), reds(cnt);
+        std::vector<std::string> names(cnt);
+        for (int k = 0; k < cnt; ++k) {
+          const int isrc = c0 + k;
+          names[k] = daw::shot_name(isrc);
+          if (names[k].empty()) throw Fail{DAW_ERR_ARG, "i too big (subroutine subname)"};
+          daw_shot_desc& d = descs[k];
+          d = daw_shot_desc{};
+          d.shot = isrc;
+          d.nt = nt;
+          d.s = s.data();
+          for (int q = 0; q < 5; ++q) d.src_tab[q] = src_tab[(isrc - 1) + (size_t)nsrc * q];
+          d.rec_tab = rec_tab.data();
+          d.nrec = nrec;
+          d.type_src = pf.type_src;
+          d.type_rec = pf.type_rec;
+          d.mu = pf.mu;
+          d.maxiter = (int)pf.maxiter;
+          d.rtol = pf.error;
+          std::memcpy(d.band, band, sizeof band);
+          data[k].resize(nd);
+          if (pf.mode == 1) {
+            read_raw(join(dir, "dataobs_org_" + names[k] + ".bin"), data[k].data(), nd);
+            d.dobs = data[k].data();
+          }
+        }
+        if (pf.mode == 0) {
+          std::vector<float*> outs(cnt);
+          for (int k = 0; k < cnt; ++k) outs[k] = data[k].data();
+          check(h, daw_submodeling_shots(h, cnt, descs.data(), outs.data()),
+                "daw_submodeling_shots");
+          for (int k = 0; k < cnt; ++k)
+            write_raw(join(dir, "dataobs_" + names[k] + ".bin"), data[k].data(), nd);
+        } else {
+          std::vector<daw_shot_out> outs(cnt);
+          for (int k = 0; k < cnt; ++k) {
+            outs[k] = daw_shot_out{};
+            if (dn) {
+              reds[k].resize((size_t)nt * dn);
+              outs[k].redatumed = reds[k].data();
+            }
+          }
+          check(h, daw_shots(h, cnt, descs.data(), outs.data()), "daw_shots");
+          for (int k = 0; k < cnt; ++k)
+            if (dn)
+              write_raw(join(dir, "dataobs_redatum_" + names[k] + ".bin"), reds[k].data(),
+                        reds[k].size());
+        }
+      }
+      return DAW_OK;
+    }
     for (int isrc = a; isrc <= b; ++isrc) {
       const std::string nm = daw::shot_name(isrc);
       if (nm.empty()) throw Fail{DAW_ERR_ARG, "i too big (subroutine subname)"};
@@ -184,30 +242,6 @@ extern "C" int daw_run_parfile(daw_handle* h, const char* workdir_c, int32_t fir
         info.log = logrows.data();
         info.log_capacity = (int)logrows.size() / 5;
         std::vector<float> datar(nd, 0.f), deltadr(nd), deltade(nd), dataesc(nd), datae(nd);
-        if (pf.mode == 1 && pf.oio != 1) {
-          // fused pipeline: no wavefield histories leave the device
-          daw_shot_desc d{};
-          d.shot = isrc;
-          d.nt = nt;
-          d.s = s.data();
-          std::memcpy(d.src_tab, src5, sizeof src5);
-          d.rec_tab = rec_tab.data();
-          d.nrec = nrec;
-          d.dobs = dobs.data();
-          d.type_src = pf.type_src;
-          d.type_rec = pf.type_rec;
-          d.mu = pf.mu;
-          d.maxiter = (int)pf.maxiter;
-          d.rtol = pf.error;
-          std::memcpy(d.band, band, sizeof band);
-          std::vector<float> red((size_t)nt * std::max(dn, 1));
-          daw_shot_out o{};
-          o.redatumed = dn ? red.data() : nullptr;
-          o.minres = info;
-          check(h, daw_shot(h, &d, &o), "daw_shot");
-          if (dn) write_raw(join(dir, "dataobs_redatum_" + nm + ".bin"), red.data(), (size_t)nt * dn);
-          continue;
-        }
         std::vector<float> wr, we;
         if (pf.mode == 1) {
           wr.resize(ni * nt);

@@ -147,6 +147,7 @@ struct ShotCtx {
   // simulation state
   float *px = nullptr, *pz = nullptr, *vx = nullptr, *vz = nullptr, *p = nullptr;
   void* hist = nullptr;
+  int hist_steps = 0;  // steps the history buffer holds
   unsigned* amax = nullptr;
   double* d_cost = nullptr;
   // operator I/O for the current application
@@ -397,6 +398,7 @@ void alloc_state(daw_handle* h, ShotCtx& c, int slot, int nt_alloc, bool fp16) {
   c.vz = st5 + 3 * ne;
   c.p = st5 + 4 * ne;
   c.hist = h->pool.get(p + "hist", hist_bytes_per_step(h, fp16) * (size_t)nt_alloc);
+  c.hist_steps = nt_alloc;
   c.amax = h->pool.get_t<unsigned>(p + "amax", (size_t)(nt_alloc + 1) * 3 * kAmaxSlots);
   c.d_cost = h->pool.get_t<double>(p + "cost", 1);
 }
@@ -522,6 +524,7 @@ struct Batch {
   TmaMaps* d_maps = nullptr;
   std::vector<ShotDevice> h_shots;
   int max_nt = 0, max_rec = 0, max_datum = 0;
+  bool no_datum = false;  // forward-only batches: no datum gathers
   int slot0 = 0;
 };
 
@@ -543,7 +546,7 @@ void fill_shot_devices(daw_handle* h, Batch& b, int mode) {
     d.type_rec = c.type_rec;
     d.active = c.active ? 1 : 0;
     d.rec = c.rec;
-    if (h->ndatum > 0) d.datum = h->datum;  // else n = 0: no datum gathers
+    if (h->ndatum > 0 && !b.no_datum) d.datum = h->datum;  // else n = 0: no datum gathers
     d.cost = nullptr;
     if (mode == FM_FWD) {
       d.amp = c.d_s;
@@ -551,7 +554,7 @@ void fill_shot_devices(daw_handle* h, Batch& b, int mode) {
       d.inj = c.srcmap;
       d.out = c.d_datar;
       d.out_reverse = 0;
-      d.red = h->ndatum > 0 ? c.d_redF : nullptr;
+      d.red = h->ndatum > 0 && !b.no_datum ? c.d_redF : nullptr;
       d.wf = c.d_wf;
       d.wf_acc = 0;
     } else if (mode == FM_STAGE_A) {
@@ -575,7 +578,7 @@ void fill_shot_devices(daw_handle* h, Batch& b, int mode) {
     for (size_t i = 0; i < b.shots.size(); ++i) {
       const ShotCtx& c = *b.shots[i];
       if (!tma_encode_maps(h->g, c.vx, c.vz, c.px, c.pz, c.p, h->md.kap, c.hist,
-                           h->opt.history_fp16, hist_ld(h), c.nt, &maps[i]))
+                           h->opt.history_fp16, hist_ld(h), c.hist_steps, &maps[i]))
         throw DawError{DAW_ERR_CUDA, "cuTensorMapEncodeTiled failed"};
     }
     b.d_maps = static_cast<TmaMaps*>(
@@ -701,7 +704,7 @@ void clear_amax(daw_handle* h, Batch& b) {
 void batch_forward(daw_handle* h, Batch& b) {
   if (!h->opt.fused) {
     for (ShotCtx* c : b.shots)
-      plain_forward(h, *c, c->d_datar, c->d_wf, h->ndatum ? c->d_redF : nullptr);
+      plain_forward(h, *c, c->d_datar, c->d_wf, h->ndatum && !b.no_datum ? c->d_redF : nullptr);
     return;
   }
   for (ShotCtx* c : b.shots) {
@@ -1026,9 +1029,10 @@ size_t shot_bytes(const daw_handle* h, int nt, int nr, bool fp16, bool want_wf) 
 }
 
 void prepare_shot(daw_handle* h, ShotCtx& c, const daw_shot_desc& d, int slot, bool want_wf,
-                  bool fp16) {
+                  bool fp16, bool forward_only = false) {
   const Grid& g = h->g;
-  if (d.nt <= 0 || d.nrec < 0 || !d.s || (d.nrec > 0 && (!d.rec_tab || !d.dobs)))
+  if (d.nt <= 0 || d.nrec < 0 || !d.s ||
+      (d.nrec > 0 && (!d.rec_tab || (!forward_only && !d.dobs))))
     throw DawError{DAW_ERR_ARG, "shot " + std::to_string(d.shot) + ": bad descriptor"};
   c = ShotCtx();
   c.shot = d.shot;
@@ -1054,7 +1058,7 @@ void prepare_shot(daw_handle* h, ShotCtx& c, const daw_shot_desc& d, int slot, b
   c.d_redf = c.d_red + nd;
   c.d_s = c.d_redf + nd + nd;
   upload(c.d_s, d.s, (size_t)d.nt * 4, h->st);
-  upload(c.d_dobs, d.dobs, n * 4, h->st);
+  if (d.dobs) upload(c.d_dobs, d.dobs, n * 4, h->st);
   c.rec = make_stations(h, h->pool, p + "rec", d.rec_tab, d.nrec);
   c.recmap = make_map(h, h->pool, p + "recmap", d.rec_tab, d.nrec);
   int32_t s5[5];
@@ -1063,7 +1067,81 @@ void prepare_shot(daw_handle* h, ShotCtx& c, const daw_shot_desc& d, int slot, b
   c.srcmap = make_map(h, h->pool, p + "srcmap", s5, 1);
   c.d_wf = want_wf ? h->pool.get_t<float>(p + "wf", g.int_elems() * (size_t)d.nt) : nullptr;
   c.d_ampT = h->pool.get_t<float>(p + "ampT", std::max<size_t>(n, 1));
-  alloc_state(h, c, slot, d.nt, fp16);
+  // forward-only shots keep no history: one step is allocated so that the
+  // (unused) history tensor map describes real memory
+  alloc_state(h, c, slot, forward_only ? 1 : d.nt, fp16);
+}
+
+// Device bytes of one forward-only shot (state, one history step, data, maps).
+size_t shot_bytes_forward(const daw_handle* h, int nt, int nr) {
+  const Grid& g = h->g;
+  size_t b = 5 * g.ext_elems() * 4 + hist_bytes_per_step(h, true) * 2 + 2 * 3 * kAmaxSlots * 4;
+  b += ((size_t)8 * nt * nr + (size_t)5 * nt * std::max(h->ndatum, 1) + nt) * 4;
+  b += (size_t)nr * kTile * 12 * 2 + (size_t)g.n2e * 16 * 2;
+  return b;
+}
+
+// Batched forward modelling (mode 0): many shots per launch, receiver data
+// only.  At most kForwardBatch shots per batch.
+constexpr int kForwardBatch = 64;
+void run_forward_shots(daw_handle* h, int n, const daw_shot_desc* descs, float* const* sis) {
+  require_model(h);
+  if (n <= 0) return;
+  int max_nt = 0, max_nr = 0;
+  for (int i = 0; i < n; ++i) {
+    max_nt = std::max(max_nt, descs[i].nt);
+    max_nr = std::max(max_nr, descs[i].nrec);
+    if (descs[i].nrec > 0 && !sis[i])
+      throw DawError{DAW_ERR_ARG, "daw_submodeling_shots: output " + std::to_string(i) + " is NULL"};
+  }
+  int S = std::min(n, kForwardBatch);
+  if (h->opt.fused) {
+    size_t free_b = 0, total_b = 0;
+    CK(cudaMemGetInfo(&free_b, &total_b));
+    const size_t per = shot_bytes_forward(h, max_nt, max_nr);
+    const size_t avail = (size_t)((double)(free_b + h->pool.total) * 0.92);
+    S = std::min<int>(S, (int)(avail / std::max<size_t>(per, 1)));
+    if (S < 1) throw DawError{DAW_ERR_OOM, "HBM admission refused for a forward shot"};
+  } else {
+    S = 1;
+  }
+  if (h->opt.max_batch > 0) S = std::min(S, h->opt.max_batch);
+  drop_graphs(h);
+  for (int first = 0; first < n; first += S) {
+    const int cnt = std::min(S, n - first);
+    std::vector<ShotCtx> ctx(cnt);
+    Batch b;
+    b.slot0 = 0;
+    b.no_datum = true;
+    for (int i = 0; i < cnt; ++i) {
+      prepare_shot(h, ctx[i], descs[first + i], i, false, h->opt.history_fp16 != 0, true);
+      ctx[i].active = true;
+      b.shots.push_back(&ctx[i]);
+      b.max_nt = std::max(b.max_nt, ctx[i].nt);
+      b.max_rec = std::max(b.max_rec, ctx[i].nr);
+    }
+    b.max_datum = 0;
+    if (h->opt.fused)
+      b.d_shots = static_cast<ShotDevice*>(h->pool.get("batch.shots0", cnt * sizeof(ShotDevice)));
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    CK(cudaEventRecord(e0, h->st));
+    batch_forward(h, b);
+    CK(cudaEventRecord(e1, h->st));
+    for (int i = 0; i < cnt; ++i)
+      if (ctx[i].nr > 0)
+        download(sis[first + i], ctx[i].d_datar, (size_t)ctx[i].nt * ctx[i].nr * sizeof(float),
+                 h->st);
+    sync(h);
+    float ms = 0;
+    CK(cudaEventElapsedTime(&ms, e0, e1));
+    h->tim.forward_ms += ms;
+    h->tim.total_ms += ms;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    drop_graphs(h);
+  }
 }
 
 void run_pipeline(daw_handle* h, Batch& b) {
@@ -1607,6 +1685,15 @@ int daw_filmartin2d(daw_handle* h, const float* in, int32_t nr, int32_t nt, floa
     *flow = band[0]; *fhig = band[1]; *llow = band[2]; *lhig = band[3];
     download(out, dout, n * 4, h->st);
     sync(h);
+  });
+}
+
+int daw_submodeling_shots(daw_handle* h, int32_t n, const daw_shot_desc* descs,
+                          float* const* sis) {
+  return guarded(h, [&] {
+    if (n < 0 || (n > 0 && (!descs || !sis)))
+      throw DawError{DAW_ERR_ARG, "daw_submodeling_shots: bad arguments"};
+    run_forward_shots(h, n, descs, sis);
   });
 }
 

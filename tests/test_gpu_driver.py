@@ -1,0 +1,94 @@
+"""The reference workflow through daw_run_parfile: redatum.par, raw float32
+models and wavelet, the acquisition text file, and the output files of modes
+0 and 1 (sub_redatum_DAW.f90).  The driver batches shots; its files must
+equal the C-ABI calls on the same inputs bit for bit."""
+import os
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def case(pkg):
+    from daw_b200 import synthetic
+    w = synthetic.small()
+    return dict(w=w, s=w.wavelet())
+
+
+def _raw(path, a):
+    np.asarray(a, np.float32).ravel(order="F").tofile(path)
+
+
+def _acqui(path, src_pos, rec_pos):
+    with open(path, "w") as f:
+        f.write(f"{len(src_pos)} {len(rec_pos)}\n")
+        for z, x in list(src_pos) + list(rec_pos):
+            f.write(f"{float(z):.9g} {float(x):.9g}\n")
+
+
+def _par(path, w, mode, nsrc_maxiter, datum_file=None):
+    band = w.band
+    lines = [
+        f"{mode}                    !modeling",
+        "vtrue.bin vinit.bin      !velocity model",
+        "acqui.txt                !acquisition",
+        "wavelet.bin              !wavelet file",
+        f"{band[0]} {band[1]} {band[2]} {band[3]}   !filter",
+        f"{w.n1} {w.n2} {w.npml} {w.h} {w.nt} {w.dt} {w.dt}   !n1 n2 npml h nt dt dto",
+        "0 0                      !source/receiver type",
+        f"{w.ofs}                  !ofs",
+        f"{w.mu}                  !penalty",
+        "0                        !oio",
+        f"0.0 {nsrc_maxiter}      !error maxiter",
+    ]
+    if datum_file:
+        lines.append(datum_file)
+    with open(path, "w") as f:
+        f.write("\n".join(lines) + "\n")
+
+
+def test_parfile_modes_0_and_1(pkg, case, tmp_path):
+    w = case["w"]
+    d = str(tmp_path)
+    src_pos = np.array([w.src_pos[0], w.src_pos[0] + np.array([0.0, 3 * w.h]),
+                        w.src_pos[0] + np.array([0.0, 7 * w.h])], np.float32)
+    rec_pos = np.asarray(w.rec_pos[0], np.float32)
+    hh = np.float32(w.h) * np.float32(w.h)
+    s_file = (case["s"] * hh).astype(np.float32)
+    s_api = (s_file / hh).astype(np.float32)  # the driver's division (main_redatum_DAW.f90:111)
+    _raw(os.path.join(d, "vtrue.bin"), w.vtrue)
+    _raw(os.path.join(d, "vinit.bin"), w.c0)
+    _raw(os.path.join(d, "wavelet.bin"), s_file)
+    _acqui(os.path.join(d, "acqui.txt"), src_pos, rec_pos)
+    _acqui(os.path.join(d, "datum.txt"), [], np.asarray(w.datum_pos, np.float32))
+    rec = pkg.subacqui(rec_pos, w.h, w.npml, w.ofs)
+    srcs = [pkg.subacqui(src_pos[i:i + 1], w.h, w.npml, w.ofs)[0] for i in range(3)]
+    with pkg.Handle(0, preset="mixed") as h:
+        # mode 0: observed data of every shot in the true model
+        _par(os.path.join(d, "redatum.par"), w, 0, w.maxiter)
+        h.run_parfile(d)
+        h.set_model(w.vtrue, w.npml, w.h, w.dt, w.ofs)
+        dobs = []
+        for i in range(3):
+            got = np.fromfile(os.path.join(d, f"dataobs_{i + 1:05d}.bin"), np.float32)
+            ref, _ = h.submodeling(s_api, srcs[i], rec)
+            assert np.array_equal(got.reshape(ref.shape, order="F"), ref)
+            dobs.append(ref)
+            os.replace(os.path.join(d, f"dataobs_{i + 1:05d}.bin"),
+                       os.path.join(d, f"dataobs_org_{i + 1:05d}.bin"))
+        # mode 1 with the datum record: redatumed data of every shot
+        _par(os.path.join(d, "redatum.par"), w, 1, w.maxiter, "datum.txt")
+        h.run_parfile(d)
+        h.set_model(w.c0, w.npml, w.h, w.dt, w.ofs)
+        ird = pkg.subacqui(np.asarray(w.datum_pos, np.float32), w.h, w.npml, w.ofs)
+        h.set_datum(ird)
+        outs = h.shots([dict(s=s_api, nt=w.nt, src=srcs[i], rec=rec, dobs=dobs[i], mu=w.mu,
+                             maxiter=w.maxiter, rtol=0.0, band=w.band) for i in range(3)],
+                       outputs=("redatumed",))
+        for i in range(3):
+            got = np.fromfile(os.path.join(d, f"dataobs_redatum_{i + 1:05d}.bin"), np.float32)
+            ref = outs[i]["redatumed"]
+            assert np.abs(ref).max() > 0
+            assert np.array_equal(got.reshape(ref.shape, order="F"), ref)
