@@ -195,6 +195,7 @@ struct daw_handle {
   int staged_ready = 0;
   // TMA kernels: persistent grid sizes and the bounded-wait error flag
   int persist_p = 0, persist_v = 0;
+  int persist_v_mode[8] = {};  // velocity kernel grid per (mode, FP16 history)
   unsigned* d_err = nullptr;
 };
 
@@ -631,6 +632,7 @@ void stop_clock(daw_handle* h, SimClock& clk, Batch& b, int mode) {
 void run_fused(daw_handle* h, Batch& b, int mode) {
   const Grid& g = h->g;
   FusedLaunch L = launch_of(h, b);
+  L.persist_v = h->persist_v_mode[mode * 2 + (L.hist_fp16 ? 1 : 0)];
   L.nparam = std::min<int>((int)b.shots.size(), FusedLaunch::kParamShots);
   unsigned long long phash = 1469598103934665603ull;  // FNV-1a of the per-shot parameters
   auto mix = [&](unsigned long long v) { phash = (phash ^ v) * 1099511628211ull; };
@@ -1377,7 +1379,7 @@ int daw_create(daw_handle** out, int32_t device) {
     delete h;
     return DAW_ERR_CUDA;
   }
-  tma_prepare(&h->persist_p, &h->persist_v);
+  tma_prepare(&h->persist_p, &h->persist_v, h->persist_v_mode);
   if (cudaMalloc(&h->d_err, sizeof(unsigned)) != cudaSuccess ||
       cudaMemset(h->d_err, 0, sizeof(unsigned)) != cudaSuccess || cudaGetLastError() != cudaSuccess) {
     cudaGetLastError();

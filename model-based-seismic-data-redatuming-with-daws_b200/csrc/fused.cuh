@@ -78,7 +78,10 @@ struct FusedLaunch {
 
 // TMA kernels (stencil_tma.cu)
 int tma_tiles(const Grid& g);
-void tma_prepare(int* persist_p, int* persist_v);
+// Persistent grid sizes: the pressure kernels' (one for all modes), the
+// velocity kernels' minimum, and the velocity kernel's per instantiation
+// (index mode * 2 + fp16).
+void tma_prepare(int* persist_p, int* persist_v, int* persist_v_mode);
 // One bounded mbarrier wait that nothing completes: raises kErrTimeout in
 // *err after `budget` cycles.
 void tma_wait_selftest(unsigned* err, long long budget, cudaStream_t st);

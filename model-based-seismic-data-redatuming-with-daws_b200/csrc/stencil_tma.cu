@@ -68,7 +68,9 @@ __host__ __device__ constexpr int v_stage(int mode, bool fp16) {
   return kVStage + ((mode == FM_STAGE_B || mode == FM_STAGE_B_ES) ? 2 * hist_box(fp16) : 0);
 }
 constexpr size_t p_smem(int mode, bool fp16) { return 2 * p_stage(mode, fp16) + 16 + kAmpBytes; }
-constexpr size_t v_smem(int mode, bool fp16) { return 2 * v_stage(mode, fp16) + 128 + kGatherBytes; }
+// The gathers' products (kGatherBytes) reuse the stage buffers after the tiles.
+constexpr size_t v_smem(int mode, bool fp16) { return 2 * v_stage(mode, fp16) + 128; }
+static_assert(2 * kVStage >= kGatherBytes, "gather products fit in the stage buffers");
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return (uint32_t)__cvta_generic_to_shared(p);
@@ -739,15 +741,18 @@ __global__ void __launch_bounds__(kThreadsT, 2)
 // Velocity kernel.  The receiver / datum gathers (8 stations per unit) run
 // after the stencil tiles, on the CTAs that drew one tile fewer.
 // ---------------------------------------------------------------------------
+// 3 CTAs per SM in the forward and stage-A modes (80 registers); the stage-B
+// modes keep 2 (their heavier body and tile count balance better at 2).
 template <int MODE, bool FP16>
-__global__ void __launch_bounds__(kThreadsT, 2)
+__global__ void __launch_bounds__(kThreadsT,
+                                  (MODE == FM_STAGE_B || MODE == FM_STAGE_B_ES) ? 2 : 3)
     k_tma_v(const Grid g, const ModelDev m, const FusedLaunch L, const int it, const int ntiles,
             const int ngb_per_shot) {
   constexpr bool kB = (MODE == FM_STAGE_B || MODE == FM_STAGE_B_ES);
   constexpr int kStage = v_stage(MODE, FP16);
   extern __shared__ __align__(128) unsigned char smem[];
   uint64_t* bar = reinterpret_cast<uint64_t*>(smem + 2 * kStage);
-  float* prod = reinterpret_cast<float*>(smem + 2 * kStage + 128);
+  float* prod = reinterpret_cast<float*>(smem);  // gathers run after the tiles
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   if (tid == 0) {
     bar_init(&bar[0]);
@@ -1034,9 +1039,11 @@ int occupancy(K kernel, size_t smem) {
 }
 
 template <int MODE, bool FP16>
-void prep_mode(int* pp, int* pv) {
+void prep_mode(int* pp, int* pv, int* pv_mode) {
   *pp = std::min(*pp, occupancy(k_tma_p<MODE, FP16>, p_smem(MODE, FP16)));
-  *pv = std::min(*pv, occupancy(k_tma_v<MODE, FP16>, v_smem(MODE, FP16)));
+  const int ov = occupancy(k_tma_v<MODE, FP16>, v_smem(MODE, FP16));
+  *pv = std::min(*pv, ov);
+  pv_mode[MODE * 2 + (FP16 ? 1 : 0)] = ov;
 }
 
 // Self-test of the failure path of the bounded waits: thread 0 waits on an
@@ -1063,21 +1070,23 @@ int tma_tiles(const Grid& g) { return ((g.n1e + TR - 1) / TR) * ((g.n2e + TC - 1
 // Persistent grid sizes (CTAs resident on all SMs) and the dynamic shared
 // memory opt-in of every instantiation; call once per device, outside graph
 // capture.
-void tma_prepare(int* persist_p, int* persist_v) {
+void tma_prepare(int* persist_p, int* persist_v, int* persist_v_mode) {
   int dev = 0, sms = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   int op = 64, ov = 64;
-  prep_mode<FM_FWD, true>(&op, &ov);
-  prep_mode<FM_FWD, false>(&op, &ov);
-  prep_mode<FM_STAGE_A, true>(&op, &ov);
-  prep_mode<FM_STAGE_A, false>(&op, &ov);
-  prep_mode<FM_STAGE_B, true>(&op, &ov);
-  prep_mode<FM_STAGE_B, false>(&op, &ov);
-  prep_mode<FM_STAGE_B_ES, true>(&op, &ov);
-  prep_mode<FM_STAGE_B_ES, false>(&op, &ov);
+  int pvm[8] = {};
+  prep_mode<FM_FWD, true>(&op, &ov, pvm);
+  prep_mode<FM_FWD, false>(&op, &ov, pvm);
+  prep_mode<FM_STAGE_A, true>(&op, &ov, pvm);
+  prep_mode<FM_STAGE_A, false>(&op, &ov, pvm);
+  prep_mode<FM_STAGE_B, true>(&op, &ov, pvm);
+  prep_mode<FM_STAGE_B, false>(&op, &ov, pvm);
+  prep_mode<FM_STAGE_B_ES, true>(&op, &ov, pvm);
+  prep_mode<FM_STAGE_B_ES, false>(&op, &ov, pvm);
   *persist_p = std::max(1, op) * sms;
   *persist_v = std::max(1, ov) * sms;
+  for (int i = 0; i < 8; ++i) persist_v_mode[i] = std::max(1, pvm[i]) * sms;
 }
 
 void tma_p_step(const Grid& g, const ModelDev& m, const FusedLaunch& L, int mode, int it,
