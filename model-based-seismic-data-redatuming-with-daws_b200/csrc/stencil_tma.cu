@@ -648,7 +648,15 @@ __global__ void __launch_bounds__(kThreadsT, 2)
         const float* PZf = PXf + TR * TC;
         const float* KAf = PZf + TR * TC;
         const int2* rp2 = reinterpret_cast<const int2*>(sd.inj.rowptr);
-        for (int pass = 0; pass < TR; pass += 32) {
+        // rows to finish per column: the band's row pairs inside the tile
+        int rows = 0;
+#pragma unroll
+        for (int j = 0; j < CPT; ++j) {
+          const int blo = __shfl_sync(kAll, bl, j), bhi = __shfl_sync(kAll, bh, j);
+          const int lo = max(blo & ~1, id.r0), hi = min(bhi | 1, rlast);
+          if (blo <= rlast && bhi >= id.r0) rows = max(rows, hi - lo + 1);
+        }
+        for (int pass = 0; pass < rows; pass += 32) {
           int rr[CPT], e0[CPT], e1[CPT];
           bool on[CPT];
 #pragma unroll
