@@ -364,7 +364,8 @@ __global__ void __launch_bounds__(kThreadsT, 2)
     tma_2d(st + kPVX + kPVZ + kPF, &mp->pz, id.r0, id.c0, &bar[s]);
     tma_2d(st + kPVX + kPVZ + 2 * kPF, &mp->kap, id.r0, id.c0, &bar[s]);
     if (kB) {  // pressure history of the time-reversed step
-      const int ic = L.shots[id.shot].nt - it + 1;
+      // record length from the kernel parameters (no load on the issuing thread's path)
+      const int ic = (id.shot < L.nparam ? L.shot_nt[id.shot] : L.shots[id.shot].nt) - it + 1;
       tma_3d(st + kPStage, &mp->hist, id.r0 - hbase, id.c0 - g.npml, (ic - 1) * 3, &bar[s],
              l2_evict_first());
     }
@@ -778,7 +779,8 @@ __global__ void __launch_bounds__(kThreadsT,
     tma_2d(st + kVP, &mp->vx16, id.r0, id.c0, &bar[s]);
     tma_2d(st + kVP + kPF, &mp->vz16, id.r0, id.c0, &bar[s]);
     if (kB) {  // velocity histories of the time-reversed step
-      const int ic = L.shots[id.shot].nt - it + 1;
+      // record length from the kernel parameters (no load on the issuing thread's path)
+      const int ic = (id.shot < L.nparam ? L.shot_nt[id.shot] : L.shots[id.shot].nt) - it + 1;
       const uint64_t pol = l2_evict_first();
       tma_3d(st + kVStage, &mp->hist, id.r0 - hbase, id.c0 - g.npml, (ic - 1) * 3 + 1, &bar[s],
              pol);
