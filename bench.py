@@ -184,6 +184,18 @@ def cpu_baseline(max_procs=None):
 
 
 # ---------------------------------------------------------------------------
+def op_steps_per_application(nt, window):
+    """Time steps of one G G^T application: stage A (nt steps + the history
+    flush step) and stage B (nt steps); with history windows of `window`
+    steps, stage A also re-runs every window but the last, each with its own
+    flush step."""
+    if window <= 0 or window >= nt:
+        return 2 * nt + 1
+    nwin = -(-nt // window)
+    last = nt - (nwin - 1) * window
+    return nt + (nt - last) + (2 * nwin - 1) + nt
+
+
 def roofline(pkg, tim, nshots, w, steps_per_op):
     peaks = json.load(open(PEAKS)) if os.path.exists(PEAKS) else {}
     peak = peaks.get("hbm_gbs", 6650.0)
@@ -222,7 +234,7 @@ def run_ours(args):
     # this rank's shots: the first B of its para_range block of the 50 shots
     ids = ranks.rank_shots(len(w.src_pos), B, rank, world)
     reduced = w.nt != 7500 or w.maxiter != 20  # profiling-sized variant
-    h = pkg.Handle(local, preset="mixed")
+    h = pkg.Handle(local, preset="mixed", checkpoint=args.checkpoint)
     shots = shot_dicts(pkg, h, w, ids, model_dobs=not reduced)
     h.stage_shots(shots)
     for _ in range(args.warmup):
@@ -242,7 +254,7 @@ def run_ours(args):
     # G G^T applications per shot: the shift's (1), the reference's unused one
     # (1) and one per MINRES iteration (rtol 0: all run); each is stage A (nt
     # steps + the history flush step) followed by stage B (nt steps)
-    op_steps = (2 * w.nt + 1) * (2 + w.maxiter) * args.steps
+    op_steps = op_steps_per_application(w.nt, args.checkpoint) * (2 + w.maxiter) * args.steps
     roof = roofline(pkg, tim, B, w, op_steps)
     # accuracy of the mixed path against the FP32-history fused path on the same shots
     out_mixed = h.fetch_staged(outputs=("deltade", "redatumed"))
@@ -299,6 +311,8 @@ def run_ours(args):
                                    + (" (reduced profiling variant with dobs = 0, not the "
                                       "benchmark)" if reduced else ""),
                        "shots_per_step_per_gpu": B, "parallelism": f"shots x{world} (no collective)",
+                       "stage_a_history": (f"windows of {args.checkpoint} steps (checkpointed)"
+                                           if 0 < args.checkpoint < w.nt else "whole record"),
                        "l2": "working set (78 GB FP16 history per shot) far exceeds L2"},
             "clocks": clk.summary(),
             "e2e": e2e,
@@ -355,7 +369,11 @@ def main():
     ap.add_argument("--nt", type=int, default=7500)
     ap.add_argument("--maxiter", type=int, default=None)
     ap.add_argument("--no-e2e", action="store_true")
+    # stage-A history in windows of K steps (checkpointed; one shot per launch)
+    ap.add_argument("--checkpoint", type=int, default=0)
     args = ap.parse_args()
+    if args.checkpoint > 0 and args.batch != 1:
+        ap.error("--checkpoint runs one shot per launch: give --batch 1")
     if args.impl == "reference":
         run_reference(args)
     else:

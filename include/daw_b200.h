@@ -62,9 +62,18 @@ enum daw_option {
   DAW_OPT_SKIP_DEAD_OP = 5,  /* 1 = skip MINRES's unused initial operator
                                 application (minresModule.f90:132); default 0 */
   DAW_OPT_MAX_BATCH = 6,     /* upper bound on shots per batched launch (0 = auto) */
-  DAW_OPT_CHUNK = 7          /* fused kernels: 0 = TMA-pipelined persistent kernels
+  DAW_OPT_CHUNK = 7,         /* fused kernels: 0 = TMA-pipelined persistent kernels
                                 (default); 1, 2 or 4 = register kernels with that
                                 many columns per thread */
+  DAW_OPT_CHECKPOINT = 8     /* fused kernels: stage-A history window in time steps.
+                                0 (default) = the whole record when a shot's history
+                                fits in device memory, else the largest window that
+                                fits; K > 0 = windows of K steps.  A shot with a
+                                window runs alone: stage A saves its state before each
+                                window and is re-run over each window (but the last)
+                                from that state while stage B consumes the windows in
+                                reverse order.  No counterpart in the reference, which
+                                keeps whole histories. */
 };
 
 /* Handle lifetime ------------------------------------------------------- */

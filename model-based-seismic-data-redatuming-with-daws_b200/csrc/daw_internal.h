@@ -116,6 +116,7 @@ struct Options {
   int skip_dead_op = 0;
   int max_batch = 0;
   int chunk = 0;
+  int checkpoint = 0;  // stage-A history window in steps (0 = automatic)
 };
 
 }  // namespace daw

@@ -148,6 +148,12 @@ struct ShotCtx {
   float *px = nullptr, *pz = nullptr, *vx = nullptr, *vz = nullptr, *p = nullptr;
   void* hist = nullptr;
   int hist_steps = 0;  // steps the history buffer holds
+  // Checkpointed stage A (hist_win > 0): the history buffer holds a window of
+  // hist_win steps; ckpt holds the states before windows 1 .. nwin-1 and st_b
+  // stage B's own state.
+  int hist_win = 0;
+  float* ckpt = nullptr;
+  float* st_b = nullptr;
   unsigned* amax = nullptr;
   double* d_cost = nullptr;
   // operator I/O for the current application
@@ -389,7 +395,9 @@ size_t hist_bytes_per_step(const daw_handle* h, bool fp16) {
   return (size_t)3 * hist_ld(h) * h->g.n2 * (fp16 ? 2 : 4);
 }
 
-void alloc_state(daw_handle* h, ShotCtx& c, int slot, int nt_alloc, bool fp16) {
+// State and history of a shot of nt_alloc steps; win > 0 (less than
+// nt_alloc) keeps the history in windows of win steps.
+void alloc_state(daw_handle* h, ShotCtx& c, int slot, int nt_alloc, bool fp16, int win = 0) {
   const size_t ne = h->g.ext_elems();
   const std::string p = "slot" + std::to_string(slot) + ".";
   float* st5 = h->pool.get_t<float>(p + "state", 5 * ne);
@@ -398,10 +406,17 @@ void alloc_state(daw_handle* h, ShotCtx& c, int slot, int nt_alloc, bool fp16) {
   c.vx = st5 + 2 * ne;
   c.vz = st5 + 3 * ne;
   c.p = st5 + 4 * ne;
-  c.hist = h->pool.get(p + "hist", hist_bytes_per_step(h, fp16) * (size_t)nt_alloc);
-  c.hist_steps = nt_alloc;
-  c.amax = h->pool.get_t<unsigned>(p + "amax", (size_t)(nt_alloc + 1) * 3 * kAmaxSlots);
+  const int hs = (win > 0 && win < nt_alloc) ? win : nt_alloc;
+  c.hist = h->pool.get(p + "hist", hist_bytes_per_step(h, fp16) * (size_t)hs);
+  c.hist_steps = hs;
+  c.amax = h->pool.get_t<unsigned>(p + "amax", (size_t)(hs + 1) * 3 * kAmaxSlots);
   c.d_cost = h->pool.get_t<double>(p + "cost", 1);
+  c.hist_win = hs < nt_alloc ? hs : 0;
+  if (c.hist_win) {
+    const size_t nwin = (size_t)(nt_alloc + hs - 1) / hs;
+    c.st_b = h->pool.get_t<float>(p + "stateB", 5 * ne);
+    c.ckpt = h->pool.get_t<float>(p + "ckpt", (nwin - 1) * 5 * ne);
+  }
 }
 
 void zero_state(daw_handle* h, ShotCtx& c) {
@@ -529,11 +544,19 @@ struct Batch {
   int slot0 = 0;
 };
 
+// A window of a checkpointed shot's record: steps s0+1 .. s0+len.
+struct Window {
+  int s0 = 0, len = 0;
+};
+
 // 0: TMA-pipelined persistent kernels (default); 1, 2, 4: register kernels
 // with that many columns per thread.
 int chunk_of(const daw_handle* h) { return h->opt.chunk; }
 
-void fill_shot_devices(daw_handle* h, Batch& b, int mode) {
+// Device descriptors (and tensor maps) of the batch's shots for `mode`.  With
+// a window, stage A sees the window as a record of w->len steps whose
+// amplitudes start at step w->s0 + 1.
+void fill_shot_devices(daw_handle* h, Batch& b, int mode, const Window* w = nullptr) {
   b.h_shots.resize(b.shots.size());
   for (size_t i = 0; i < b.shots.size(); ++i) {
     ShotCtx& c = *b.shots[i];
@@ -559,9 +582,10 @@ void fill_shot_devices(daw_handle* h, Batch& b, int mode) {
       d.wf = c.d_wf;
       d.wf_acc = 0;
     } else if (mode == FM_STAGE_A) {
-      d.amp = c.op_in;
+      d.amp = c.op_in + (w ? w->s0 : 0);
       d.amp_stride = c.nt;
       d.inj = c.recmap;
+      if (w) d.nt = w->len;
     } else {
       d.out = c.op_out;
       d.out_reverse = c.op_reverse;
@@ -620,17 +644,22 @@ void check_device_error(daw_handle* h) {
 // Runs `nsteps` steps of `mode`, captured once per batch/mode in a CUDA
 // graph when enabled (kernel arguments are constant; per-shot pointers live in
 // the device-side ShotDevice array, refreshed before each replay).
-void stop_clock(daw_handle* h, SimClock& clk, Batch& b, int mode) {
+void stop_clock(daw_handle* h, SimClock& clk, Batch& b, int mode, const Window* w) {
   double shot_steps = 0;
   for (ShotCtx* c : b.shots)
-    if (c->active) shot_steps += c->nt;
+    if (c->active) shot_steps += w ? w->len : c->nt;
   double* ms = mode == FM_FWD ? &h->tim.sim_fwd_ms : mode == FM_STAGE_A ? &h->tim.sim_a_ms : &h->tim.sim_b_ms;
   double* st = mode == FM_FWD ? &h->tim.steps_fwd : mode == FM_STAGE_A ? &h->tim.steps_a : &h->tim.steps_b;
-  clk.stop(ms, st, b.max_nt, shot_steps);
+  clk.stop(ms, st, w ? w->len : b.max_nt, shot_steps);
 }
 
-void run_fused(daw_handle* h, Batch& b, int mode) {
+// With a window (one shot, checkpointed stage A): stage A runs the window as a
+// record of w->len steps; stage B runs the record steps that read the
+// window's history, nt-s0-len+1 .. nt-s0, with history slot 0 = step s0+1.
+// Windowed runs are launched directly (no graph).
+void run_fused(daw_handle* h, Batch& b, int mode, const Window* w = nullptr) {
   const Grid& g = h->g;
+  if (w && b.shots.size() != 1) throw DawError{DAW_ERR_STATE, "a windowed run holds one shot"};
   FusedLaunch L = launch_of(h, b);
   L.persist_v = h->persist_v_mode[mode * 2 + (L.hist_fp16 ? 1 : 0)];
   L.nparam = std::min<int>((int)b.shots.size(), FusedLaunch::kParamShots);
@@ -639,28 +668,41 @@ void run_fused(daw_handle* h, Batch& b, int mode) {
   for (int i = 0; i < FusedLaunch::kParamShots; ++i) {
     const ShotCtx* c = i < L.nparam ? b.shots[i] : nullptr;
     L.shot_amax[i] = c ? c->amax : nullptr;
-    L.shot_amp[i] = !c ? nullptr : mode == FM_FWD ? c->d_s : mode == FM_STAGE_A ? c->d_ampT : nullptr;
-    L.shot_nt[i] = c ? c->nt : 0;
+    L.shot_amp[i] = !c ? nullptr
+                    : mode == FM_FWD ? c->d_s
+                    : mode == FM_STAGE_A ? c->d_ampT + (w ? (size_t)w->s0 * c->nr : 0)
+                                         : nullptr;
+    L.shot_nt[i] = !c ? 0 : (w && mode == FM_STAGE_A) ? w->len : c->nt;
     L.shot_nsta[i] = !c ? 0 : mode == FM_FWD ? 1 : mode == FM_STAGE_A ? c->nr : 0;
     mix((unsigned long long)(uintptr_t)L.shot_amax[i]);
     mix((unsigned long long)(uintptr_t)L.shot_amp[i]);
     mix((unsigned long long)L.shot_nt[i] << 32 | (unsigned)L.shot_nsta[i]);
   }
-  const int last = (mode == FM_STAGE_A) ? b.max_nt + 1 : b.max_nt;  // +1: history flush
+  // steps first..last; the velocity kernel runs for it <= nt_v
+  int first = 1, nt_v = b.max_nt;
+  if (w && mode == FM_STAGE_A) {
+    nt_v = w->len;
+  } else if (w) {
+    first = b.max_nt - w->s0 - w->len + 1;
+    nt_v = b.max_nt - w->s0;
+    L.hist_step0 = w->s0;
+  }
+  const int last = (mode == FM_STAGE_A) ? nt_v + 1 : nt_v;  // +1: history flush
   const bool tma = L.chunk == 0;
   auto body = [&]() {
-    for (int it = 1; it <= last; ++it) {
+    for (int it = first; it <= last; ++it) {
       if (tma) {
         tma_p_step(g, h->md, L, mode, it, h->st);
-        if (it <= b.max_nt) tma_v_step(g, h->md, L, mode, it, h->st);
+        if (it <= nt_v) tma_v_step(g, h->md, L, mode, it, h->st);
       } else {
         fused_p_step(g, h->md, L, mode, it, h->st);
-        if (it <= b.max_nt) fused_v_step(g, h->md, L, mode, it, h->st);
+        if (it <= nt_v) fused_v_step(g, h->md, L, mode, it, h->st);
       }
     }
   };
-  const long long launches = 2LL * b.max_nt + (mode == FM_STAGE_A ? 1 : 0);
-  if (h->opt.graph) {
+  const int nsteps = nt_v - first + 1;
+  const long long launches = 2LL * nsteps + (mode == FM_STAGE_A ? 1 : 0);
+  if (h->opt.graph && !w) {
     char key[256];
     std::snprintf(key, sizeof key, "m%d.n%d.s%zu.p%p.q%p.c%d.f%d.r%d.d%d.h%llx", mode, b.max_nt,
                   b.shots.size(), (void*)b.d_shots, (void*)b.d_maps, L.chunk, L.hist_fp16,
@@ -678,21 +720,22 @@ void run_fused(daw_handle* h, Batch& b, int mode) {
     }
     SimClock clk(h);
     CK(cudaGraphLaunch(it->second, h->st));
-    stop_clock(h, clk, b, mode);
+    stop_clock(h, clk, b, mode, w);
   } else {
     SimClock clk(h);
     body();
-    stop_clock(h, clk, b, mode);
+    stop_clock(h, clk, b, mode, w);
   }
   check_launch("fused steps");
   check_device_error(h);
   h->tim.kernel_launches += launches;
-  for (ShotCtx* c : b.shots)
-    if (c->active) h->tim.point_updates += (double)c->nt * g.n1e * g.n2e;
-  if (mode != FM_FWD)
-    for (ShotCtx* c : b.shots)
-      if (c->active)
-        h->tim.hist_bytes += (double)c->nt * 3 * g.int_elems() * (h->opt.history_fp16 ? 2 : 4);
+  for (ShotCtx* c : b.shots) {
+    if (!c->active) continue;
+    const double steps = w ? w->len : c->nt;
+    h->tim.point_updates += steps * g.n1e * g.n2e;
+    if (mode != FM_FWD)
+      h->tim.hist_bytes += steps * 3 * g.int_elems() * (h->opt.history_fp16 ? 2 : 4);
+  }
 }
 
 void clear_amax(daw_handle* h, Batch& b) {
@@ -719,6 +762,73 @@ void batch_forward(daw_handle* h, Batch& b) {
   run_fused(h, b, FM_FWD);
 }
 
+// G G^T (stage A + stage B) of one shot whose stage-A history is kept in
+// windows of K = hist_win steps.  Stage A runs once over the record, window
+// by window, saving its state before each window; the last window's history
+// stays in the buffer.  Stage B then takes the windows in reverse order and,
+// before each window but the last, re-runs stage A over that window from the
+// saved state.  Stage A's kernels see a window as a record of its own length
+// whose amplitudes start at the window's first step, and the history flush
+// step leaves the state unchanged, so every history value comes from the same
+// operations as in the whole-record run: the outputs are equal bit for bit
+// (the FP64 cost sum aside, whose order is unspecified in both).
+void shot_operator_windowed(daw_handle* h, Batch& b, bool esource) {
+  ShotCtx& c = *b.shots[0];
+  if (!c.active) return;
+  const size_t ne = h->g.ext_elems(), state_bytes = 5 * ne * sizeof(float);
+  const int K = c.hist_win, nwin = (c.nt + K - 1) / K;
+  float* const st_a = c.px;  // the slot's state [5][ne]
+  auto use_state = [&](float* s5) {
+    c.px = s5; c.pz = s5 + ne; c.vx = s5 + 2 * ne; c.vz = s5 + 3 * ne; c.p = s5 + 4 * ne;
+  };
+  struct Restore {  // the ShotCtx points at stage A's state again on every exit
+    std::function<void()> f;
+    ~Restore() { f(); }
+  } restore{[&] { use_state(st_a); }};
+  auto window = [&](int w) { return Window{w * K, std::min(K, c.nt - w * K)}; };
+  auto stage_a = [&](int w) {
+    const Window win = window(w);
+    CK(cudaMemsetAsync(c.amax, 0, (size_t)(win.len + 1) * 3 * kAmaxSlots * sizeof(unsigned), h->st));
+    fill_shot_devices(h, b, FM_STAGE_A, &win);
+    run_fused(h, b, FM_STAGE_A, &win);
+  };
+  if (c.nr > 0) {
+    transpose_traces(c.op_in, c.d_ampT, c.nt, c.nr, h->st);
+    h->tim.kernel_launches += 1;
+  }
+  zero_state(h, c);
+  for (int w = 0; w < nwin; ++w) {
+    if (w > 0)
+      CK(cudaMemcpyAsync(c.ckpt + (size_t)(w - 1) * 5 * ne, st_a, state_bytes,
+                         cudaMemcpyDeviceToDevice, h->st));
+    stage_a(w);
+  }
+  const int mode = esource ? FM_STAGE_B_ES : FM_STAGE_B;
+  use_state(c.st_b);
+  zero_state(h, c);
+  CK(cudaMemsetAsync(c.op_out, 0, (size_t)c.nt * c.nr * sizeof(float), h->st));
+  if (esource && h->ndatum)
+    CK(cudaMemsetAsync(c.d_redE, 0, (size_t)c.nt * h->ndatum * sizeof(float), h->st));
+  for (int w = nwin - 1; w >= 0; --w) {
+    if (w < nwin - 1) {
+      use_state(st_a);
+      if (w == 0)
+        zero_state(h, c);
+      else
+        CK(cudaMemcpyAsync(st_a, c.ckpt + (size_t)(w - 1) * 5 * ne, state_bytes,
+                           cudaMemcpyDeviceToDevice, h->st));
+      stage_a(w);
+      use_state(c.st_b);
+    }
+    const Window win = window(w);
+    if (esource && c.d_cost)
+      history_cost(c.hist, h->opt.history_fp16, c.amax, win.len, h->g.n1, h->g.n2, hist_ld(h),
+                   h->g.npml - h->g.hist_base(), (size_t)hist_ld(h) * h->g.n2, c.d_cost, h->st);
+    fill_shot_devices(h, b, mode, &win);
+    run_fused(h, b, mode, &win);
+  }
+}
+
 // Stage A + stage B.  esource: final simulation (interior 2..n-1 pressure
 // source, datum gather, optional wavefield accumulation and cost).
 void batch_operator(daw_handle* h, Batch& b, bool esource) {
@@ -735,6 +845,13 @@ void batch_operator(daw_handle* h, Batch& b, bool esource) {
     }
     return;
   }
+  for (ShotCtx* c : b.shots)
+    if (c->hist_win > 0) {
+      if (b.shots.size() != 1)
+        throw DawError{DAW_ERR_STATE, "a shot with a windowed history runs alone"};
+      shot_operator_windowed(h, b, esource);
+      return;
+    }
   for (ShotCtx* c : b.shots) {
     if (!c->active) continue;
     zero_state(h, *c);
@@ -1018,11 +1135,17 @@ void run_filter(daw_handle* h, const float* d_in, float* d_out, int nt, int nr, 
 // ---------------------------------------------------------------------------
 // Shot preparation and the batched pipeline
 // ---------------------------------------------------------------------------
-size_t shot_bytes(const daw_handle* h, int nt, int nr, bool fp16, bool want_wf) {
+// Device bytes of one shot.  win > 0 (less than nt): the history is kept in
+// windows of win steps, and the states saved before the later windows plus
+// stage B's own state take the place of the rest of the history.
+size_t shot_bytes(const daw_handle* h, int nt, int nr, bool fp16, bool want_wf, int win = 0) {
   const Grid& g = h->g;
-  size_t b = 5 * g.ext_elems() * 4;                       // state
-  b += hist_bytes_per_step(h, fp16) * (size_t)nt;          // history
-  b += (size_t)(nt + 1) * 3 * kAmaxSlots * 4;
+  const size_t state = 5 * g.ext_elems() * 4;
+  const int hs = (win > 0 && win < nt) ? win : nt;
+  size_t b = state;                                        // state
+  b += hist_bytes_per_step(h, fp16) * (size_t)hs;          // history (window)
+  b += (size_t)(hs + 1) * 3 * kAmaxSlots * 4;
+  if (hs < nt) b += state * (size_t)((nt + hs - 1) / hs);  // saved states + stage-B state
   b += (size_t)(8 + 7) * nt * nr * 4;                      // MINRES + data arrays
   b += (size_t)6 * nt * std::max(h->ndatum, 1) * 4;        // datum gathers
   if (want_wf) b += g.int_elems() * (size_t)nt * 4;
@@ -1031,7 +1154,7 @@ size_t shot_bytes(const daw_handle* h, int nt, int nr, bool fp16, bool want_wf) 
 }
 
 void prepare_shot(daw_handle* h, ShotCtx& c, const daw_shot_desc& d, int slot, bool want_wf,
-                  bool fp16, bool forward_only = false) {
+                  bool fp16, bool forward_only = false, int win = 0) {
   const Grid& g = h->g;
   if (d.nt <= 0 || d.nrec < 0 || !d.s ||
       (d.nrec > 0 && (!d.rec_tab || (!forward_only && !d.dobs))))
@@ -1071,7 +1194,7 @@ void prepare_shot(daw_handle* h, ShotCtx& c, const daw_shot_desc& d, int slot, b
   c.d_ampT = h->pool.get_t<float>(p + "ampT", std::max<size_t>(n, 1));
   // forward-only shots keep no history: one step is allocated so that the
   // (unused) history tensor map describes real memory
-  alloc_state(h, c, slot, forward_only ? 1 : d.nt, fp16);
+  alloc_state(h, c, slot, forward_only ? 1 : d.nt, fp16, forward_only ? 0 : win);
 }
 
 // Device bytes of one forward-only shot (state, one history step, data, maps).
@@ -1240,18 +1363,44 @@ void fetch_outputs(daw_handle* h, ShotCtx& c, daw_shot_out* o) {
   sync(h);
 }
 
-int admit_batch(daw_handle* h, int n, const daw_shot_desc* d, bool want_wf) {
-  if (!h->opt.fused) return 1;
+// Device bytes a batch may use: free memory plus the handle's reusable
+// buffers, less a margin.
+size_t admission_bytes(daw_handle* h) {
   size_t free_b = 0, total_b = 0;
   CK(cudaMemGetInfo(&free_b, &total_b));
-  size_t held = h->pool.total;  // reusable
+  return (size_t)((double)(free_b + h->pool.total) * 0.92);
+}
+
+// Stage-A history window of a shot of nt steps (fused kernels only): 0 keeps
+// the whole history; DAW_OPT_CHECKPOINT = K > 0 asks for windows of K steps;
+// 0 picks the largest window that fits when the whole history does not.
+int history_window(daw_handle* h, int nt, int nr, bool want_wf, size_t avail) {
+  if (!h->opt.fused) return 0;
+  if (h->opt.checkpoint > 0) return h->opt.checkpoint < nt ? h->opt.checkpoint : 0;
+  const bool fp16 = h->opt.history_fp16 != 0;
+  if (shot_bytes(h, nt, nr, fp16, want_wf) <= avail) return 0;
+  for (int k = nt - 1; k >= 1; --k)
+    if (shot_bytes(h, nt, nr, fp16, want_wf, k) <= avail) return k;
+  throw DawError{DAW_ERR_OOM, "HBM admission refused: one shot needs " +
+                                  std::to_string(shot_bytes(h, nt, nr, fp16, want_wf, 1)) +
+                                  " bytes with the smallest history window, " +
+                                  std::to_string(avail) + " available"};
+}
+
+// Shots per batch, and in *win the stage-A history window (a shot with a
+// window runs alone).
+int admit_batch(daw_handle* h, int n, const daw_shot_desc* d, bool want_wf, int* win) {
+  *win = 0;
+  if (!h->opt.fused) return 1;
   int max_nt = 0, max_nr = 0;
   for (int i = 0; i < n; ++i) {
     max_nt = std::max(max_nt, d[i].nt);
     max_nr = std::max(max_nr, d[i].nrec);
   }
+  const size_t avail = admission_bytes(h);
+  *win = history_window(h, max_nt, max_nr, want_wf, avail);
+  if (*win > 0) return 1;
   const size_t per = shot_bytes(h, max_nt, max_nr, h->opt.history_fp16, want_wf);
-  const size_t avail = (size_t)((double)(free_b + held) * 0.92);
   int s = (int)(avail / std::max<size_t>(per, 1));
   if (s < 1)
     throw DawError{DAW_ERR_OOM, "HBM admission refused: one shot needs " + std::to_string(per) +
@@ -1266,7 +1415,8 @@ void run_shots(daw_handle* h, int n, const daw_shot_desc* descs, daw_shot_out* o
   if (n <= 0) return;
   bool want_wf = false;
   for (int i = 0; i < n; ++i) want_wf |= (outs && outs[i].wavefield_exd != nullptr);
-  const int S = admit_batch(h, n, descs, want_wf);
+  int win = 0;
+  const int S = admit_batch(h, n, descs, want_wf, &win);
   // Free per-slot buffers beyond the admitted batch size and stale graphs.
   drop_graphs(h);
   for (int first = 0; first < n; first += S) {
@@ -1276,7 +1426,7 @@ void run_shots(daw_handle* h, int n, const daw_shot_desc* descs, daw_shot_out* o
     b.slot0 = 0;
     for (int i = 0; i < cnt; ++i) {
       prepare_shot(h, ctx[i], descs[first + i], i, outs && outs[first + i].wavefield_exd,
-                   h->opt.history_fp16 != 0);
+                   h->opt.history_fp16 != 0, false, win);
       b.shots.push_back(&ctx[i]);
     }
     run_pipeline(h, b);
@@ -1286,8 +1436,9 @@ void run_shots(daw_handle* h, int n, const daw_shot_desc* descs, daw_shot_out* o
 }
 
 // Single-shot operator helpers for the reference-routine mirrors.
+// forward_only: no stage-A history (one step allocated for the unused map).
 ShotCtx& single_ctx(daw_handle* h, ShotCtx& c, int nt, const int32_t* ir, int nr, int type_rec,
-                    bool want_wf) {
+                    bool want_wf, bool forward_only = false) {
   if (nt <= 0 || nr < 0 || (nr > 0 && !ir)) throw DawError{DAW_ERR_ARG, "bad nt/nr/table"};
   check_table(h, ir, nr, true, "ir");
   c = ShotCtx();
@@ -1307,7 +1458,8 @@ ShotCtx& single_ctx(daw_handle* h, ShotCtx& c, int nt, const int32_t* ir, int nr
   c.recmap = make_map(h, h->pool, p + "recmap", ir, nr);
   c.d_wf = want_wf ? h->pool.get_t<float>(p + "wf", h->g.int_elems() * (size_t)nt) : nullptr;
   c.d_ampT = h->pool.get_t<float>(p + "ampT", std::max<size_t>(n, 1));
-  alloc_state(h, c, 0, nt, h->opt.history_fp16 != 0 && h->opt.fused != 0);
+  const int win = forward_only ? 0 : history_window(h, nt, nr, want_wf, admission_bytes(h));
+  alloc_state(h, c, 0, forward_only ? 1 : nt, h->opt.history_fp16 != 0 && h->opt.fused != 0, win);
   return c;
 }
 
@@ -1430,6 +1582,10 @@ int daw_set_option(daw_handle* h, int32_t key, double value) {
           throw DawError{DAW_ERR_ARG, "points per thread must be 1, 2 or 4 (0 = default)"};
         h->opt.chunk = v;
         break;
+      case DAW_OPT_CHECKPOINT:
+        if (v < 0) throw DawError{DAW_ERR_ARG, "history window must be >= 0 (0 = automatic)"};
+        h->opt.checkpoint = v;
+        break;
       default: throw DawError{DAW_ERR_ARG, "unknown option"};
     }
     if (!h->opt.fused && h->opt.history_fp16)
@@ -1450,6 +1606,7 @@ int daw_get_option(const daw_handle* h, int32_t key, double* value) {
     case DAW_OPT_SKIP_DEAD_OP: *value = o.skip_dead_op; break;
     case DAW_OPT_MAX_BATCH: *value = o.max_batch; break;
     case DAW_OPT_CHUNK: *value = o.chunk; break;
+    case DAW_OPT_CHECKPOINT: *value = o.checkpoint; break;
     default: return DAW_ERR_ARG;
   }
   return DAW_OK;
@@ -1528,7 +1685,7 @@ int daw_submodeling(daw_handle* h, const float* s, int32_t nt, const int32_t* is
     require_model(h);
     if (!s || !is5 || !sis) throw DawError{DAW_ERR_ARG, "daw_submodeling: null argument"};
     ShotCtx c;
-    single_ctx(h, c, nt, ir, nr, type_rec, wavefield != nullptr);
+    single_ctx(h, c, nt, ir, nr, type_rec, wavefield != nullptr, true);
     c.type_src = type_src;
     check_table(h, is5, 1, true, "is");
     std::memcpy(c.src5, is5, sizeof c.src5);
@@ -1738,13 +1895,15 @@ int daw_stage_shots(daw_handle* h, int32_t n, const daw_shot_desc* descs) {
   return guarded(h, [&] {
     require_model(h);
     if (n <= 0 || !descs) throw DawError{DAW_ERR_ARG, "daw_stage_shots: bad arguments"};
-    const int S = admit_batch(h, n, descs, false);
+    int win = 0;
+    const int S = admit_batch(h, n, descs, false, &win);
     if (S < n)
       throw DawError{DAW_ERR_OOM, "staged shots must fit one batch (" + std::to_string(S) +
                                       " admitted of " + std::to_string(n) + ")"};
     drop_graphs(h);
     h->staged_ctx.assign(n, ShotCtx());
-    for (int i = 0; i < n; ++i) prepare_shot(h, h->staged_ctx[i], descs[i], i, false, h->opt.history_fp16 != 0);
+    for (int i = 0; i < n; ++i)
+      prepare_shot(h, h->staged_ctx[i], descs[i], i, false, h->opt.history_fp16 != 0, false, win);
     sync(h);
     h->staged_ready = n;
   });

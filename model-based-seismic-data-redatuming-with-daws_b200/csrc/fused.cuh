@@ -63,6 +63,9 @@ struct FusedLaunch {
   const TmaMaps* maps;      // device array, one per shot (TMA kernels)
   unsigned* err;            // raised by a bounded wait that ran out
   int persist_p, persist_v; // persistent grid sizes of the TMA kernels
+  // Stage B: the history buffer holds record steps hist_step0+1 .. (a window
+  // of a checkpointed stage A) in its slots 0, 1, ...; 0 = the whole record.
+  int hist_step0;
   // Per-shot pointers passed as kernel parameters for the first kParamShots
   // shots, so that a CTA's per-shot set-up needs one round of loads: the
   // max-|x| slots, the injection amplitudes in step-major order

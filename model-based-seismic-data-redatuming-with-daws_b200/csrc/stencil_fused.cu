@@ -175,6 +175,7 @@ __global__ void __launch_bounds__(kThreads)
   const bool r1 = ok1 && i1 + 1 >= npml && i1 + 1 < npml + g.n1;
   const int h1 = i1 - g.hist_base();  // history row of i1 (even)
   const int ic = nt - it + 1;
+  const int hs = ic - 1 - L.hist_step0;  // stage B: history slot of step ic
 
   float inv_vx = 1.f, inv_vz = 1.f, sc_p = 1.f;
   if (FP16) {
@@ -184,7 +185,7 @@ __global__ void __launch_bounds__(kThreads)
       inv_vz = pow2f(15 - amax_exponent(warp_amax_slots(a + 2 * kAmaxSlots)));
     }
     if (MODE == FM_STAGE_B || MODE == FM_STAGE_B_ES) {
-      const unsigned* a = sd.amax + (size_t)(ic - 1) * 3 * kAmaxSlots;
+      const unsigned* a = sd.amax + (size_t)hs * 3 * kAmaxSlots;
       sc_p = pow2f(amax_exponent(warp_amax_slots(a)) - 15);
     }
   }
@@ -225,7 +226,7 @@ __global__ void __launch_bounds__(kThreads)
   const bool s1 = r1 && i1 + 1 - npml >= slo && i1 + 1 - npml < shi1;
   void* hv_store = (MODE == FM_STAGE_A && it >= 2) ? step_base<FP16>(sd.hist, it - 2, nih) : nullptr;
   const void* hp_read = (MODE == FM_STAGE_B || MODE == FM_STAGE_B_ES)
-                            ? step_base<FP16>(sd.hist, ic - 1, nih) : nullptr;
+                            ? step_base<FP16>(sd.hist, hs, nih) : nullptr;
   unsigned lmax = 0;
 
 #pragma unroll
@@ -380,6 +381,7 @@ __global__ void __launch_bounds__(kThreads)
   const bool r1 = ok1 && i1 + 1 >= npml && i1 + 1 < npml + g.n1;
   const int h1 = i1 - g.hist_base();
   const int ic = nt - it + 1;
+  const int hs = ic - 1 - L.hist_step0;  // stage B: history slot of step ic
   float inv_p = 1.f, sc_vx = 1.f, sc_vz = 1.f;
   if (FP16) {
     if (MODE == FM_STAGE_A) {
@@ -387,7 +389,7 @@ __global__ void __launch_bounds__(kThreads)
       inv_p = pow2f(15 - amax_exponent(warp_amax_slots(a)));
     }
     if (MODE == FM_STAGE_B || MODE == FM_STAGE_B_ES) {
-      const unsigned* a = sd.amax + (size_t)(ic - 1) * 3 * kAmaxSlots;
+      const unsigned* a = sd.amax + (size_t)hs * 3 * kAmaxSlots;
       sc_vx = pow2f(amax_exponent(warp_amax_slots(a + kAmaxSlots)) - 15);
       sc_vz = pow2f(amax_exponent(warp_amax_slots(a + 2 * kAmaxSlots)) - 15);
     }
@@ -397,7 +399,7 @@ __global__ void __launch_bounds__(kThreads)
   float* __restrict__ vza = sd.vz;
   void* hp_store = (MODE == FM_STAGE_A) ? step_base<FP16>(sd.hist, it - 1, nih) : nullptr;
   const void* hv_read = (MODE == FM_STAGE_B || MODE == FM_STAGE_B_ES)
-                            ? step_base<FP16>(sd.hist, ic - 1, nih) : nullptr;
+                            ? step_base<FP16>(sd.hist, hs, nih) : nullptr;
   // ---- loads
   float2 qp[NP + 3];  // p at columns c0-1 .. c0+NP+1
 #pragma unroll

@@ -366,7 +366,8 @@ __global__ void __launch_bounds__(kThreadsT, 2)
     if (kB) {  // pressure history of the time-reversed step
       // record length from the kernel parameters (no load on the issuing thread's path)
       const int ic = (id.shot < L.nparam ? L.shot_nt[id.shot] : L.shots[id.shot].nt) - it + 1;
-      tma_3d(st + kPStage, &mp->hist, id.r0 - hbase, id.c0 - g.npml, (ic - 1) * 3, &bar[s],
+      const int hs = ic - 1 - L.hist_step0;  // history slot of step ic
+      tma_3d(st + kPStage, &mp->hist, id.r0 - hbase, id.c0 - g.npml, hs * 3, &bar[s],
              l2_evict_first());
     }
   };
@@ -409,7 +410,8 @@ __global__ void __launch_bounds__(kThreadsT, 2)
           s0v = am[(size_t)(it - 2) * 3 * kAmaxSlots + kAmaxSlots + lane];
           s1v = am[(size_t)(it - 2) * 3 * kAmaxSlots + 2 * kAmaxSlots + lane];
         }
-        if (kB && FP16 && it <= ntc) s0v = am[(size_t)(ntc - it) * 3 * kAmaxSlots + lane];
+        if (kB && FP16 && it <= ntc)
+          s0v = am[(size_t)(ntc - it - L.hist_step0) * 3 * kAmaxSlots + lane];
         constexpr int kPer = kAmpMax / kThreadsT;
         float av[kPer];
         const bool want_amps = (MODE == FM_STAGE_A || MODE == FM_FWD) && it <= ntc &&
@@ -455,7 +457,8 @@ __global__ void __launch_bounds__(kThreadsT, 2)
           }
         }
         if (live && kB && FP16)
-          sc_p = pow2f(amax_exponent(warp_amax_slots(sd.amax + (size_t)(nt - it) * 3 * kAmaxSlots)) - 15);
+          sc_p = pow2f(amax_exponent(warp_amax_slots(
+                           sd.amax + (size_t)(nt - it - L.hist_step0) * 3 * kAmaxSlots)) - 15);
         amp_smem = sd.inj.nsta <= kAmpMax;
         if (do_inj && amp_smem) stage_amp(amp_s, sd.amp + (it - 1), sd.amp_stride, sd.inj.nsta);
       }
@@ -782,10 +785,10 @@ __global__ void __launch_bounds__(kThreadsT,
       // record length from the kernel parameters (no load on the issuing thread's path)
       const int ic = (id.shot < L.nparam ? L.shot_nt[id.shot] : L.shots[id.shot].nt) - it + 1;
       const uint64_t pol = l2_evict_first();
-      tma_3d(st + kVStage, &mp->hist, id.r0 - hbase, id.c0 - g.npml, (ic - 1) * 3 + 1, &bar[s],
-             pol);
-      tma_3d(st + kVStage + hist_box(FP16), &mp->hist, id.r0 - hbase, id.c0 - g.npml,
-             (ic - 1) * 3 + 2, &bar[s], pol);
+      const int hs = ic - 1 - L.hist_step0;  // history slot of step ic
+      tma_3d(st + kVStage, &mp->hist, id.r0 - hbase, id.c0 - g.npml, hs * 3 + 1, &bar[s], pol);
+      tma_3d(st + kVStage + hist_box(FP16), &mp->hist, id.r0 - hbase, id.c0 - g.npml, hs * 3 + 2,
+             &bar[s], pol);
     }
   };
   const Walk wk = tile_walk(ntiles, L.nshots);
@@ -827,8 +830,8 @@ __global__ void __launch_bounds__(kThreadsT,
         const unsigned* am = L.shot_amax[cur];
         if (MODE == FM_STAGE_A && it <= ntc) s0v = am[(size_t)(it - 1) * 3 * kAmaxSlots + lane];
         if (kB && it <= ntc) {
-          s0v = am[(size_t)(ntc - it) * 3 * kAmaxSlots + kAmaxSlots + lane];
-          s1v = am[(size_t)(ntc - it) * 3 * kAmaxSlots + 2 * kAmaxSlots + lane];
+          s0v = am[(size_t)(ntc - it - L.hist_step0) * 3 * kAmaxSlots + kAmaxSlots + lane];
+          s1v = am[(size_t)(ntc - it - L.hist_step0) * 3 * kAmaxSlots + 2 * kAmaxSlots + lane];
         }
       }
       sd = L.shots[cur];
@@ -843,7 +846,7 @@ __global__ void __launch_bounds__(kThreadsT,
                                       : warp_amax_slots(sd.amax + (size_t)(it - 1) * 3 * kAmaxSlots)));
       }
       if (live && kB && FP16) {
-        const unsigned* a = sd.amax + (size_t)(sd.nt - it) * 3 * kAmaxSlots;
+        const unsigned* a = sd.amax + (size_t)(sd.nt - it - L.hist_step0) * 3 * kAmaxSlots;
         sc_vx = pow2f(amax_exponent(fast ? __reduce_max_sync(kAll, s0v)
                                          : warp_amax_slots(a + kAmaxSlots)) - 15);
         sc_vz = pow2f(amax_exponent(fast ? __reduce_max_sync(kAll, s1v)
