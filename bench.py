@@ -29,6 +29,7 @@ import signal
 import statistics
 import subprocess
 import sys
+import tempfile
 import time
 
 import numpy as np
@@ -39,7 +40,7 @@ import __graft_entry__ as entry  # noqa: E402
 
 PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
 # DRAM bytes of one G G^T time step (p + v kernels), measured by ncu on the
-# same grid and batch (profiles/k_tma_751x2301_stageA_stageB.md)
+# same grid and batch
 TRAFFIC = os.path.join(ROOT, "profiles", "k_tma_751x2301_traffic.json")
 METRIC = "shots/hour redatumed at <=1e-3 rel err vs FP64: batched mixed vs plain FP32"
 
@@ -91,11 +92,10 @@ class Clocks:
     def __init__(self, device):
         self.device = device
         self.p = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_{device}.csv")
+        self.path = os.path.join(tempfile.mkdtemp(prefix="daw_clocks_"), f"clocks_{device}.csv")
 
     def __enter__(self):
         try:
-            os.makedirs(os.path.dirname(self.path), exist_ok=True)
             self.f = open(self.path, "w")
             self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.device),
                                        f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",

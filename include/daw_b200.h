@@ -152,13 +152,17 @@ int daw_filmartin2d(daw_handle* h, const float* in, int32_t nr, int32_t nt, floa
  *   device (caller-owned); band parameters in/out as in daw_filmartin2d;
  *   stream: a cudaStream_t (NULL = legacy default stream); err: optional
  *   buffer of err_len bytes for the message of a failed call.
- * Work space is one fixed 4 MiB array that every GPU loading the library
+ * Work space is one fixed 4 MiB array that every GPU where it is set up
  * holds until exit (weights for nto <= 65536, FFT space for long traces).
- * nt above 65536 is rejected with DAW_ERR_ARG.  The first call on a device
- * takes the array's device address with that device current; make it before
- * any stream capture.  Calls share the array, so their GPU work must not
- * overlap: calls are serialised by a lock and return after their work has
- * finished on `stream`. */
+ * nt above 65536 is rejected with DAW_ERR_ARG.  The set-up, once per device
+ * with that device current, takes the array's device address; under CUDA's
+ * default lazy module loading that is also when the array and the filter
+ * kernel's code are placed on the device, which can need device memory.
+ * daw_create runs it for its device; on a device without a handle, make one
+ * call with nr = 0 (d_in and d_out may then be NULL) before the device fills
+ * up and before any stream capture.  Calls share the array, so their GPU work
+ * must not overlap: calls are serialised by a lock and return after their
+ * work has finished on `stream`. */
 int daw_filmartin2d_noalloc(const float* d_in, int32_t nr, int32_t nt, float dt, float* flow,
                             float* fhig, float* llow, float* lhig, float* d_out, void* stream,
                             char* err, int32_t err_len);

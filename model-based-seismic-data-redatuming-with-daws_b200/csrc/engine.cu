@@ -1376,8 +1376,18 @@ size_t admission_bytes(daw_handle* h) {
 // 0 picks the largest window that fits when the whole history does not.
 int history_window(daw_handle* h, int nt, int nr, bool want_wf, size_t avail) {
   if (!h->opt.fused) return 0;
-  if (h->opt.checkpoint > 0) return h->opt.checkpoint < nt ? h->opt.checkpoint : 0;
   const bool fp16 = h->opt.history_fp16 != 0;
+  if (h->opt.checkpoint > 0) {
+    // a requested window: its history plus ceil(nt/K) saved states must fit
+    const int k = h->opt.checkpoint < nt ? h->opt.checkpoint : 0;
+    const size_t need = shot_bytes(h, nt, nr, fp16, want_wf, k);
+    if (need > avail)
+      throw DawError{DAW_ERR_OOM, "HBM admission refused: one shot with history windows of " +
+                                      std::to_string(h->opt.checkpoint) + " steps needs " +
+                                      std::to_string(need) + " bytes, " + std::to_string(avail) +
+                                      " available"};
+    return k;
+  }
   if (shot_bytes(h, nt, nr, fp16, want_wf) <= avail) return 0;
   for (int k = nt - 1; k >= 1; --k)
     if (shot_bytes(h, nt, nr, fp16, want_wf, k) <= avail) return k;
@@ -1532,6 +1542,9 @@ int daw_create(daw_handle** out, int32_t device) {
     return DAW_ERR_CUDA;
   }
   tma_prepare(&h->persist_p, &h->persist_v, h->persist_v_mode);
+  // The device set-up of daw_filmartin2d_noalloc, while memory is still free
+  // (not fatal here: a failure is reported again by that entry point).
+  if (filter_noalloc_prepare(nullptr, 0) != DAW_OK) cudaGetLastError();
   if (cudaMalloc(&h->d_err, sizeof(unsigned)) != cudaSuccess ||
       cudaMemset(h->d_err, 0, sizeof(unsigned)) != cudaSuccess || cudaGetLastError() != cudaSuccess) {
     cudaGetLastError();

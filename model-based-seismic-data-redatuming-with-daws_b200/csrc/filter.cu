@@ -119,6 +119,17 @@ __global__ void __launch_bounds__(kFftThreads)
 
 }  // namespace
 
+// Loads the filter kernel's code onto the current device and sets its
+// shared-memory opt-in.  Under lazy module loading (the default since CUDA
+// 12.2) that would otherwise happen at its first launch and may need device
+// memory then.
+bool filter_preload() {
+  cudaFuncAttributes a;
+  return cudaFuncGetAttributes(&a, k_filter) == cudaSuccess &&
+         cudaFuncSetAttribute(k_filter, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)kSmemLimit) == cudaSuccess;
+}
+
 size_t filter_scratch_bytes(int nr, int nto) {
   const size_t per = (size_t)(nto / 2) * sizeof(double2);
   return per <= kSmemLimit ? 0 : per * (size_t)nr;

@@ -11,21 +11,27 @@
 // The regular entry point (daw_filmartin2d) takes host arrays and draws its
 // weights and FFT work space from a handle's device pool.  This one takes the
 // caller's device buffers for the input and output traces and keeps its work
-// space in one fixed array, g_filter_scratch below, that the library reserves
-// when it is loaded.
+// space in one fixed array, g_filter_scratch below.
 //
-// The fixed array: kScratchBytes (4 MiB) on every GPU where the library is
-// loaded, held until the process exits.  Its first kWeightBytes hold the
-// nto + 1 FP64 weights (nto <= 65536, the reference's own limit); the rest is
-// FFT work space for traces whose transform does not fit in shared memory
-// (nt > 16384), filtered a few traces per launch.  Nothing in it has to
-// start at zero: each call writes every weight and every FFT element before
-// it reads them.
+// The fixed array: kScratchBytes (4 MiB) on every GPU where it is set up,
+// held until the process exits.  Its first kWeightBytes hold the nto + 1 FP64
+// weights (nto <= 65536, the reference's own limit); the rest is FFT work
+// space for traces whose transform does not fit in shared memory
+// (nt > 16384), filtered a few traces per launch.  Nothing in it has to start
+// at zero: each call writes every weight and every FFT element before it
+// reads them.
 //
-// Host code cannot use g_filter_scratch's name as a device address.  The
-// first call on a device, with that device current, takes the address with
-// cudaGetSymbolAddress and keeps it for later calls; make that first call
-// before any stream capture.
+// Set-up, once per device, with that device current
+// (filter_noalloc_prepare): host code cannot use g_filter_scratch's name as a
+// device address, so the set-up takes the address with cudaGetSymbolAddress
+// and keeps it.  Under lazy module loading (the CUDA default since 12.2) that
+// call is also what loads this file's module onto the device and so reserves
+// the 4 MiB; the set-up loads the filter kernel's code as well.  Both can
+// need device memory, so they must not wait for a call made when HBM is
+// full: daw_create runs the set-up for its device, and a caller that never
+// creates a handle on a device makes one call with nr = 0 (buffers may then
+// be NULL) before filling the device.  A first call that finds the set-up
+// undone runs it itself; make that call before any stream capture.
 //
 // Every call shares the one array and leaves its contents behind.  Work from
 // two calls that overlapped on the GPU would race on it, so calls are
@@ -75,13 +81,49 @@ bool is_device_pointer(const void* p, int dev) {
   return a.type == cudaMemoryTypeManaged || (a.type == cudaMemoryTypeDevice && a.device == dev);
 }
 
+// The set-up of one device, under g_lock; 0 or a negative daw_status.
+int prepare_locked(int dev, char* err, int err_len) {
+  using namespace daw;
+  if (dev < 0 || dev >= kMaxDevices)
+    return fail(err, err_len, DAW_ERR_ARG, "daw_filmartin2d_noalloc: device %d outside 0..%d",
+                dev, kMaxDevices - 1);
+  if (g_scratch_ptr[dev]) return DAW_OK;
+  void* p = nullptr;
+  cudaError_t e = cudaGetSymbolAddress(&p, g_filter_scratch);
+  if (e != cudaSuccess || !p)
+    return fail(err, err_len, DAW_ERR_CUDA,
+                "daw_filmartin2d_noalloc: cudaGetSymbolAddress failed on device %d: %s", dev,
+                cudaGetErrorString(e));
+  if (!filter_preload()) {
+    e = cudaGetLastError();
+    return fail(err, err_len, DAW_ERR_CUDA,
+                "daw_filmartin2d_noalloc: loading the filter kernel failed on device %d: %s", dev,
+                cudaGetErrorString(e));
+  }
+  g_scratch_ptr[dev] = static_cast<unsigned char*>(p);
+  return DAW_OK;
+}
+
 }  // namespace
+
+namespace daw {
+int filter_noalloc_prepare(char* err, int err_len) {
+  std::lock_guard<std::mutex> guard(g_lock);
+  int dev = -1;
+  const cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess || dev < 0)
+    return fail(err, err_len, DAW_ERR_NODEV, "daw_filmartin2d_noalloc: no current device (%s)",
+                cudaGetErrorString(e));
+  return prepare_locked(dev, err, err_len);
+}
+}  // namespace daw
 
 extern "C" int daw_filmartin2d_noalloc(const float* d_in, int32_t nr, int32_t nt, float dt,
                                        float* flow, float* fhig, float* llow, float* lhig,
                                        float* d_out, void* stream, char* err, int32_t err_len) {
   using namespace daw;
-  if (!d_in || !d_out || !flow || !fhig || !llow || !lhig || nr < 0 || nt <= 0 || !(dt > 0))
+  if ((nr > 0 && (!d_in || !d_out)) || !flow || !fhig || !llow || !lhig || nr < 0 || nt <= 0 ||
+      !(dt > 0))
     return fail(err, err_len, DAW_ERR_ARG, "daw_filmartin2d_noalloc: bad arguments");
   if (nt > kMaxNto)
     return fail(err, err_len, DAW_ERR_ARG,
@@ -94,18 +136,8 @@ extern "C" int daw_filmartin2d_noalloc(const float* d_in, int32_t nr, int32_t nt
   if (e != cudaSuccess || dev < 0)
     return fail(err, err_len, DAW_ERR_NODEV, "daw_filmartin2d_noalloc: no current device (%s)",
                 cudaGetErrorString(e));
-  if (dev >= kMaxDevices)
-    return fail(err, err_len, DAW_ERR_ARG, "daw_filmartin2d_noalloc: device %d >= %d", dev,
-                kMaxDevices);
-  if (!g_scratch_ptr[dev]) {  // set-up, once per device, with that device current
-    void* p = nullptr;
-    e = cudaGetSymbolAddress(&p, g_filter_scratch);
-    if (e != cudaSuccess || !p)
-      return fail(err, err_len, DAW_ERR_CUDA,
-                  "daw_filmartin2d_noalloc: cudaGetSymbolAddress failed on device %d: %s", dev,
-                  cudaGetErrorString(e));
-    g_scratch_ptr[dev] = static_cast<unsigned char*>(p);
-  }
+  const int rc = prepare_locked(dev, err, err_len);  // once per device
+  if (rc != DAW_OK) return rc;
   if (nr > 0 && (!is_device_pointer(d_in, dev) || !is_device_pointer(d_out, dev)))
     return fail(err, err_len, DAW_ERR_ARG,
                 "daw_filmartin2d_noalloc: input and output must be device memory of the "

@@ -161,6 +161,13 @@ void transpose_traces(const float* in, float* out, int nt, int nr, cudaStream_t 
 void filter_traces(const float* in, float* out, int nt, int nr, int nto, const double* w,
                    double* scratch, cudaStream_t st);
 size_t filter_scratch_bytes(int nr, int nto);
+// Loads the filter kernel onto the current device (filter.cu).
+bool filter_preload();
+// Set-up of daw_filmartin2d_noalloc on the current device (filter_noalloc.cu):
+// takes the device address of its fixed work-space array (which loads that
+// array's module and so reserves the array) and loads the filter kernel.
+// Idempotent per device; 0 or a negative daw_status, with the message in err.
+int filter_noalloc_prepare(char* err, int err_len);
 // Padded length nto of filmartin2d (next power of two >= nt, 8..65536), or 0
 // when nt exceeds 65536 (src/minresModule.f90:503-510).
 int filter_nto(int nt);

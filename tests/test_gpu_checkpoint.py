@@ -128,3 +128,24 @@ def test_windowed_shots_bitexact(pkg, case):
         assert g["minres"]["itn"] == r["minres"]["itn"]
         assert abs(g["cost"] - r["cost"]) <= 1e-12 * abs(r["cost"])
         assert np.abs(r["redatumed"]).max() > 0
+
+
+def test_requested_window_too_small_is_refused(pkg, case):
+    """DAW_OPT_CHECKPOINT = K keeps ceil(nt/K) saved states of the extended
+    grid.  On the 751 x 2301 grid (npml 40, 40 MB per state) windows of one
+    step over 7500 steps would need ~300 GB of states: the request is refused
+    at admission with DAW_ERR_OOM, before any history is allocated, and the
+    handle keeps working."""
+    from daw_b200 import synthetic
+    w2 = synthetic.config2(nshot=1, nt=7500)
+    rec = pkg.subacqui(w2.rec_pos[0][:4], w2.h, w2.npml, w2.ofs)
+    res = np.zeros((7500, 4), np.float32, order="F")
+    with pkg.Handle(0, preset="mixed", checkpoint=1) as h:
+        h.set_model(w2.c0, w2.npml, w2.h, w2.dt, w2.ofs)
+        with pytest.raises(pkg.DawError) as e:
+            h.submodeling_adjoint_esource_data(res, rec)
+        assert e.value.code == -2, str(e.value)
+        assert "history windows of 1 steps" in str(e.value)
+        h.set_options(checkpoint=3000)
+        g = h.submodeling_adjoint_esource_data(np.zeros((300, 4), np.float32, order="F"), rec)
+        assert not g.any()

@@ -35,17 +35,22 @@ CASES = [
 ]
 
 
-def _call(L, d_in, d_out, nr, nt, dt, band, err):
+def _call(L, d_in, d_out, nr, nt, dt, band, err, stream=None):
     b = [C.c_float(v) for v in band]
     rc = L.daw_filmartin2d_noalloc(C.c_void_p(d_in), nr, nt, dt, *[C.byref(v) for v in b],
-                                   C.c_void_p(d_out), None, err, len(err))
+                                   C.c_void_p(d_out), C.c_void_p(stream), err, len(err))
     return rc, tuple(v.value for v in b)
 
 
-def test_noalloc_filter_matches_regular_entry_point_twice(pkg):
+@pytest.mark.parametrize("on_stream", [False, True])
+def test_noalloc_filter_matches_regular_entry_point_twice(pkg, on_stream):
+    """Both cases in a row; on the legacy default stream, and on a stream of
+    the caller's (a torch stream), which the call must honour: the output is
+    read back on that stream after the call returns."""
     torch = pytest.importorskip("torch")
     L = pkg.lib()
     err = C.create_string_buffer(512)
+    stream = torch.cuda.Stream(device=0) if on_stream else None
     with pkg.Handle(0, preset="mixed") as h:
         for c in CASES:
             nt, nr, dt = c["nt"], c["nr"], c["dt"]
@@ -56,12 +61,66 @@ def test_noalloc_filter_matches_regular_entry_point_twice(pkg):
             d_in = torch.from_numpy(np.ascontiguousarray(x.T)).to("cuda:0")
             d_out = torch.full_like(d_in, float("nan"))
             torch.cuda.synchronize()
-            rc, band = _call(L, d_in.data_ptr(), d_out.data_ptr(), nr, nt, dt, c["band"], err)
+            rc, band = _call(L, d_in.data_ptr(), d_out.data_ptr(), nr, nt, dt, c["band"], err,
+                             stream.cuda_stream if stream is not None else None)
             assert rc == 0, err.value.decode()
-            y = d_out.cpu().numpy().T
+            if stream is not None:
+                with torch.cuda.stream(stream):
+                    y = d_out.cpu().numpy().T
+            else:
+                y = d_out.cpu().numpy().T
             assert np.isfinite(y).all()
             assert rel_l2(y, ref) <= TOL, (nt, rel_l2(y, ref))
             assert band == ref_band
+
+
+_FRESH = r"""
+import ctypes as C, sys
+import numpy as np, torch
+sys.path.insert(0, {root!r})
+import __graft_entry__ as e
+pkg = e.load_package()
+L = pkg.lib()
+nt, nr = 20000, 5
+x = torch.randn(nr, nt, device="cuda:0")
+y = torch.empty_like(x)
+torch.cuda.synchronize()
+b = [C.c_float(v) for v in (5.0, 30.0, 5.0, 5.0)]
+err = C.create_string_buffer(256)
+def call(nr_, xin, yout):
+    return L.daw_filmartin2d_noalloc(C.c_void_p(xin), nr_, nt, 2e-3,
+                                     *[C.byref(v) for v in b], C.c_void_p(yout), None, err, 256)
+if {with_handle}:
+    h = C.c_void_p()
+    assert L.daw_create(C.byref(h), 0) == 0
+else:
+    assert call(0, None, None) == 0, err.value   # the documented set-up call
+torch.cuda.synchronize()
+free0 = torch.cuda.mem_get_info(0)[0]
+rc = call(nr, x.data_ptr(), y.data_ptr())
+torch.cuda.synchronize()
+free1 = torch.cuda.mem_get_info(0)[0]
+assert rc == 0, err.value
+assert torch.isfinite(y).all()
+print("free before", free0, "after", free1)
+assert free1 == free0, (free0, free1)
+"""
+
+
+@pytest.mark.parametrize("with_handle", [True, False])
+def test_noalloc_first_call_allocates_nothing(with_handle):
+    """In a fresh process, after daw_create on the device (or after the
+    documented set-up call with nr = 0 when no handle exists), the first
+    filtering call leaves the device's free memory unchanged: the fixed work
+    space and the filter kernel's code were placed before it.  Traces of
+    20000 samples use the FFT work space inside the fixed array."""
+    import os
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    r = subprocess.run([sys.executable, "-c", _FRESH.format(root=root, with_handle=with_handle)],
+                       capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stdout + r.stderr
 
 
 def test_noalloc_filter_rejects_traces_beyond_its_work_space(pkg):
