@@ -26,7 +26,8 @@ NVCC = os.environ.get("NVCC", shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-ffp-contract=off",
           f"-I{INCLUDE}", f"-I{CSRC}"]
-LIB_SOURCES = ["hicks.cpp", "engine.cu", "stencil_plain.cu", "stencil_fused.cu", "stencil_tma.cu", "minres.cu",
+LIB_SOURCES = ["hicks.cpp", "engine.cu", "stencil_plain.cu", "stencil_fused.cu", "stencil_tma.cu", "stencil_step.cu",
+               "minres.cu",
                "filter.cu", "filter_noalloc.cu", "driver.cpp"]
 
 

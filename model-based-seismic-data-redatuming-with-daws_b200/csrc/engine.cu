@@ -144,8 +144,19 @@ struct ShotCtx {
   float *d_redF = nullptr, *d_redE = nullptr, *d_red = nullptr, *d_redf = nullptr;
   float* d_wf = nullptr;
   float* d_ampT = nullptr;  // stage-A residual in step-major order [nt][nr]
-  // simulation state
+  // simulation state: a block of 9 fields [px, pz, vx, vz, p, px2, pz2, vx2,
+  // vz2]; the one-kernel-per-step path alternates between {px, pz, vx, vz}
+  // (set 0) and {px2, pz2, vx2, vz2} (set 1), and `par` is the set that holds
+  // the current state.
+  float* state = nullptr;
   float *px = nullptr, *pz = nullptr, *vx = nullptr, *vz = nullptr, *p = nullptr;
+  float *px2 = nullptr, *pz2 = nullptr, *vx2 = nullptr, *vz2 = nullptr;
+  int par = 0;
+  void set_state(float* s9, size_t ne) {
+    state = s9;
+    px = s9; pz = s9 + ne; vx = s9 + 2 * ne; vz = s9 + 3 * ne; p = s9 + 4 * ne;
+    px2 = s9 + 5 * ne; pz2 = s9 + 6 * ne; vx2 = s9 + 7 * ne; vz2 = s9 + 8 * ne;
+  }
   void* hist = nullptr;
   int hist_steps = 0;  // steps the history buffer holds
   // Checkpointed stage A (hist_win > 0): the history buffer holds a window of
@@ -203,6 +214,18 @@ struct daw_handle {
   int persist_p = 0, persist_v = 0;
   int persist_v_mode[8] = {};  // velocity kernel grid per (mode, FP16 history)
   unsigned* d_err = nullptr;
+  // One-kernel-per-step path: SMs, resident CTAs per SM of each (mode, FP16,
+  // tile width) [mode][fp16][tc == 32], the tile-queue counter and the
+  // autotuned configurations by (mode, FP16, grid, shots) key.
+  int sms = 0;
+  int step_occ[4][2][2] = {};
+  unsigned* d_qctr = nullptr;
+  struct Tuned {
+    int tile_cols, ctas_per_sm;
+    float us_per_step;
+  };
+  std::map<std::string, Tuned> tuned;
+  Tuned last_tuned{0, 0, 0.f};
 };
 
 namespace {
@@ -395,17 +418,16 @@ size_t hist_bytes_per_step(const daw_handle* h, bool fp16) {
   return (size_t)3 * hist_ld(h) * h->g.n2 * (fp16 ? 2 : 4);
 }
 
+// Fields of a shot's state block (see ShotCtx).
+constexpr int kStateFields = 9;
+
 // State and history of a shot of nt_alloc steps; win > 0 (less than
 // nt_alloc) keeps the history in windows of win steps.
 void alloc_state(daw_handle* h, ShotCtx& c, int slot, int nt_alloc, bool fp16, int win = 0) {
   const size_t ne = h->g.ext_elems();
   const std::string p = "slot" + std::to_string(slot) + ".";
-  float* st5 = h->pool.get_t<float>(p + "state", 5 * ne);
-  c.px = st5;
-  c.pz = st5 + ne;
-  c.vx = st5 + 2 * ne;
-  c.vz = st5 + 3 * ne;
-  c.p = st5 + 4 * ne;
+  c.set_state(h->pool.get_t<float>(p + "state", kStateFields * ne), ne);
+  c.par = 0;
   const int hs = (win > 0 && win < nt_alloc) ? win : nt_alloc;
   c.hist = h->pool.get(p + "hist", hist_bytes_per_step(h, fp16) * (size_t)hs);
   c.hist_steps = hs;
@@ -414,13 +436,14 @@ void alloc_state(daw_handle* h, ShotCtx& c, int slot, int nt_alloc, bool fp16, i
   c.hist_win = hs < nt_alloc ? hs : 0;
   if (c.hist_win) {
     const size_t nwin = (size_t)(nt_alloc + hs - 1) / hs;
-    c.st_b = h->pool.get_t<float>(p + "stateB", 5 * ne);
+    c.st_b = h->pool.get_t<float>(p + "stateB", kStateFields * ne);
     c.ckpt = h->pool.get_t<float>(p + "ckpt", (nwin - 1) * 5 * ne);
   }
 }
 
 void zero_state(daw_handle* h, ShotCtx& c) {
-  CK(cudaMemsetAsync(c.px, 0, 5 * h->g.ext_elems() * sizeof(float), h->st));
+  CK(cudaMemsetAsync(c.state, 0, kStateFields * h->g.ext_elems() * sizeof(float), h->st));
+  c.par = 0;
 }
 
 // ---------------------------------------------------------------------------
@@ -538,6 +561,7 @@ struct Batch {
   std::vector<ShotCtx*> shots;
   ShotDevice* d_shots = nullptr;
   TmaMaps* d_maps = nullptr;
+  StepMaps* d_smaps = nullptr;
   std::vector<ShotDevice> h_shots;
   int max_nt = 0, max_rec = 0, max_datum = 0;
   bool no_datum = false;  // forward-only batches: no datum gathers
@@ -552,6 +576,8 @@ struct Window {
 // 0: TMA-pipelined persistent kernels (default); 1, 2, 4: register kernels
 // with that many columns per thread.
 int chunk_of(const daw_handle* h) { return h->opt.chunk; }
+// The one-kernel-per-step TMA path (the default of the fused kernels).
+bool step_path(const daw_handle* h) { return h->opt.fused && h->opt.chunk == 0 && h->opt.step; }
 
 // Device descriptors (and tensor maps) of the batch's shots for `mode`.  With
 // a window, stage A sees the window as a record of w->len steps whose
@@ -563,6 +589,7 @@ void fill_shot_devices(daw_handle* h, Batch& b, int mode, const Window* w = null
     ShotDevice& d = b.h_shots[i];
     std::memset(&d, 0, sizeof d);
     d.px = c.px; d.pz = c.pz; d.vx = c.vx; d.vz = c.vz; d.p = c.p;
+    d.px2 = c.px2; d.pz2 = c.pz2; d.vx2 = c.vx2; d.vz2 = c.vz2;
     d.hist = c.hist;
     d.amax = c.amax;
     d.nt = c.nt;
@@ -597,7 +624,24 @@ void fill_shot_devices(daw_handle* h, Batch& b, int mode, const Window* w = null
     }
   }
   upload(b.d_shots, b.h_shots.data(), b.h_shots.size() * sizeof(ShotDevice), h->st);
-  if (chunk_of(h) == 0) {
+  if (step_path(h)) {
+    // tensor maps of every shot for both tile widths: [tile width 16 | 32][shot]
+    const size_t n = b.shots.size();
+    std::vector<StepMaps> maps(2 * n);
+    for (size_t i = 0; i < n; ++i) {
+      const ShotCtx& c = *b.shots[i];
+      float* const st[2][4] = {{c.px, c.pz, c.vx, c.vz}, {c.px2, c.pz2, c.vx2, c.vz2}};
+      for (int t = 0; t < 2; ++t)
+        if (!step_encode_maps(h->g, st, h->md.kap, c.hist, h->opt.history_fp16, hist_ld(h),
+                              c.hist_steps, t ? 32 : 16, &maps[t * n + i]))
+          throw DawError{DAW_ERR_CUDA, "cuTensorMapEncodeTiled failed"};
+    }
+    b.d_smaps = static_cast<StepMaps*>(h->pool.get(
+        "batch.smaps" + std::to_string(b.slot0) + "." + std::to_string(mode),
+        maps.size() * sizeof(StepMaps)));
+    upload(b.d_smaps, maps.data(), maps.size() * sizeof(StepMaps), h->st);
+    sync(h);  // `maps` goes out of scope
+  } else if (chunk_of(h) == 0) {
     // tensor maps of every shot's fields (the TMA kernels' operands)
     std::vector<TmaMaps> maps(b.shots.size());
     for (size_t i = 0; i < b.shots.size(); ++i) {
@@ -641,9 +685,6 @@ void check_device_error(daw_handle* h) {
   }
 }
 
-// Runs `nsteps` steps of `mode`, captured once per batch/mode in a CUDA
-// graph when enabled (kernel arguments are constant; per-shot pointers live in
-// the device-side ShotDevice array, refreshed before each replay).
 void stop_clock(daw_handle* h, SimClock& clk, Batch& b, int mode, const Window* w) {
   double shot_steps = 0;
   for (ShotCtx* c : b.shots)
@@ -653,10 +694,76 @@ void stop_clock(daw_handle* h, SimClock& clk, Batch& b, int mode, const Window* 
   clk.stop(ms, st, w ? w->len : b.max_nt, shot_steps);
 }
 
+// Autotuner of the one-kernel-per-step path: tile width (16 or 32 columns)
+// and CTAs per SM (1 .. occupancy), chosen per (mode, history precision, grid,
+// batch) by timing the run's first step with every candidate (median of 3
+// launches after a warm-up), once per handle.  The first step has no deferred
+// work and writes only the state set it is about to write anyway, and its
+// max-|x| atomics are idempotent, so the trial launches leave no trace; the
+// final esource, whose first step also accumulates into the wavefield output,
+// takes stage B's configuration (same kernel shape) and tunes as stage B.
+daw_handle::Tuned tune_step(daw_handle* h, Batch& b, int mode, FusedLaunch L, int first) {
+  const int tmode = mode == FM_STAGE_B_ES ? FM_STAGE_B : mode;
+  const int f = L.hist_fp16 ? 1 : 0;
+  char key[160];
+  std::snprintf(key, sizeof key, "m%d.f%d.g%dx%d.p%d.s%d.r%d.d%d.t%d.c%d", tmode, f, h->g.n1,
+                h->g.n2, h->g.npml, L.nshots, L.max_rec, L.max_datum, h->opt.tile_cols,
+                h->opt.ctas_per_sm);
+  auto it = h->tuned.find(key);
+  if (it != h->tuned.end()) return it->second;
+  const size_t n = b.shots.size();
+  std::vector<daw_handle::Tuned> cands;
+  for (int tc : {16, 32}) {
+    if (h->opt.tile_cols && h->opt.tile_cols != tc) continue;
+    const int occ = h->step_occ[tmode][f][tc == 32 ? 1 : 0];
+    for (int c = 1; c <= std::min(occ, 3); ++c)
+      if (!h->opt.ctas_per_sm || h->opt.ctas_per_sm == c) cands.push_back({tc, c, 0.f});
+  }
+  if (cands.empty())
+    throw DawError{DAW_ERR_CUDA, "no resident configuration of the step kernel"};
+  daw_handle::Tuned best = cands[0];
+  if (cands.size() > 1) {
+    float best_us = 1e30f;
+    for (auto& cd : cands) {
+      FusedLaunch T = L;
+      T.tile_cols = cd.tile_cols;
+      T.smaps = b.d_smaps + (cd.tile_cols == 32 ? n : 0);
+      const int grid = cd.ctas_per_sm * h->sms;
+      float ms[3];
+      for (int r = 0; r < 4; ++r) {
+        CK(cudaMemsetAsync(h->d_qctr, 0, sizeof(unsigned), h->st));
+        if (r > 0) CK(cudaEventRecord(h->ev0, h->st));
+        step_launch(h->g, h->md, T, tmode, first, grid, h->st);
+        if (r > 0) {
+          CK(cudaEventRecord(h->ev1, h->st));
+          CK(cudaEventSynchronize(h->ev1));
+          CK(cudaEventElapsedTime(&ms[r - 1], h->ev0, h->ev1));
+        }
+      }
+      check_launch("step kernel (tuning)");
+      std::sort(ms, ms + 3);
+      cd.us_per_step = ms[1] * 1e3f;
+      if (cd.us_per_step < best_us) {
+        best_us = cd.us_per_step;
+        best = cd;
+      }
+    }
+    h->tim.kernel_launches += 4 * (long long)cands.size();
+  }
+  h->tuned[key] = best;
+  return best;
+}
+
+// Runs `nsteps` steps of `mode`, captured once per batch/mode in a CUDA
+// graph when enabled (kernel arguments are constant; per-shot pointers live in
+// the device-side ShotDevice array, refreshed before each replay).
+//
 // With a window (one shot, checkpointed stage A): stage A runs the window as a
 // record of w->len steps; stage B runs the record steps that read the
 // window's history, nt-s0-len+1 .. nt-s0, with history slot 0 = step s0+1.
-// Windowed runs are launched directly (no graph).
+// The split kernels launch windowed runs directly; the one-kernel-per-step
+// path captures them in graphs too, keyed by the window's first step, length
+// and history offset and by the state set the run starts from.
 void run_fused(daw_handle* h, Batch& b, int mode, const Window* w = nullptr) {
   const Grid& g = h->g;
   if (w && b.shots.size() != 1) throw DawError{DAW_ERR_STATE, "a windowed run holds one shot"};
@@ -687,9 +794,36 @@ void run_fused(daw_handle* h, Batch& b, int mode, const Window* w = nullptr) {
     nt_v = b.max_nt - w->s0;
     L.hist_step0 = w->s0;
   }
-  const int last = (mode == FM_STAGE_A) ? nt_v + 1 : nt_v;  // +1: history flush
+  const bool step = step_path(h);
+  // the step path's extra launch does the last step's deferred work; the
+  // split kernels' extra stage-A launch flushes its history
+  const int last = step ? nt_v + 1 : (mode == FM_STAGE_A) ? nt_v + 1 : nt_v;
   const bool tma = L.chunk == 0;
+  int grid = 0;
+  if (step) {
+    int par0 = -1;
+    for (ShotCtx* c : b.shots) {
+      if (!c->active) continue;
+      if (par0 >= 0 && c->par != par0)
+        throw DawError{DAW_ERR_STATE, "shots of a batch start from different state sets"};
+      par0 = c->par;
+    }
+    L.par0 = std::max(par0, 0);
+    L.first = first;
+    L.qctr = h->d_qctr;
+    L.ngath = mode == FM_STAGE_A ? 0 : (L.max_rec + (b.no_datum ? 0 : L.max_datum) + 7) / 8;
+    const daw_handle::Tuned t = tune_step(h, b, mode, L, first);
+    h->last_tuned = t;
+    L.tile_cols = t.tile_cols;
+    L.smaps = b.d_smaps + (t.tile_cols == 32 ? b.shots.size() : 0);
+    grid = t.ctas_per_sm * h->sms;
+  }
   auto body = [&]() {
+    if (step) {
+      CK(cudaMemsetAsync(h->d_qctr, 0, sizeof(unsigned), h->st));
+      for (int it = first; it <= last; ++it) step_launch(g, h->md, L, mode, it, grid, h->st);
+      return;
+    }
     for (int it = first; it <= last; ++it) {
       if (tma) {
         tma_p_step(g, h->md, L, mode, it, h->st);
@@ -701,12 +835,15 @@ void run_fused(daw_handle* h, Batch& b, int mode, const Window* w = nullptr) {
     }
   };
   const int nsteps = nt_v - first + 1;
-  const long long launches = 2LL * nsteps + (mode == FM_STAGE_A ? 1 : 0);
-  if (h->opt.graph && !w) {
-    char key[256];
-    std::snprintf(key, sizeof key, "m%d.n%d.s%zu.p%p.q%p.c%d.f%d.r%d.d%d.h%llx", mode, b.max_nt,
-                  b.shots.size(), (void*)b.d_shots, (void*)b.d_maps, L.chunk, L.hist_fp16,
-                  L.max_rec, L.max_datum, phash);
+  const long long launches = step ? (long long)nsteps + 1
+                                  : 2LL * nsteps + (mode == FM_STAGE_A ? 1 : 0);
+  if (h->opt.graph && (!w || step)) {
+    char key[320];
+    std::snprintf(key, sizeof key,
+                  "m%d.n%d.s%zu.p%p.q%p.z%p.c%d.f%d.r%d.d%d.h%llx.w%d.%d.%d.%d.%d.%d.%d",
+                  mode, b.max_nt, b.shots.size(), (void*)b.d_shots, (void*)b.d_maps,
+                  (void*)b.d_smaps, L.chunk, L.hist_fp16, L.max_rec, L.max_datum, phash, step,
+                  first, last, L.hist_step0, L.par0, L.tile_cols, grid);
     auto it = h->graphs.find(key);
     if (it == h->graphs.end()) {
       cudaGraph_t graph;
@@ -731,10 +868,11 @@ void run_fused(daw_handle* h, Batch& b, int mode, const Window* w = nullptr) {
   h->tim.kernel_launches += launches;
   for (ShotCtx* c : b.shots) {
     if (!c->active) continue;
-    const double steps = w ? w->len : c->nt;
-    h->tim.point_updates += steps * g.n1e * g.n2e;
+    const int steps = w ? (mode == FM_STAGE_A ? w->len : nt_v - first + 1) : c->nt;
+    if (step) c->par = (c->par + steps) & 1;  // the set holding the state after the run
+    h->tim.point_updates += (double)steps * g.n1e * g.n2e;
     if (mode != FM_FWD)
-      h->tim.hist_bytes += steps * 3 * g.int_elems() * (h->opt.history_fp16 ? 2 : 4);
+      h->tim.hist_bytes += (double)steps * 3 * g.int_elems() * (h->opt.history_fp16 ? 2 : 4);
   }
 }
 
@@ -775,16 +913,22 @@ void batch_forward(daw_handle* h, Batch& b) {
 void shot_operator_windowed(daw_handle* h, Batch& b, bool esource) {
   ShotCtx& c = *b.shots[0];
   if (!c.active) return;
-  const size_t ne = h->g.ext_elems(), state_bytes = 5 * ne * sizeof(float);
+  const size_t ne = h->g.ext_elems();
+  // a saved state: the four fields of the current set (one-kernel-per-step
+  // path) or px, pz, vx, vz, p (split kernels); ckpt slots hold 5 fields
+  const bool step = step_path(h);
+  const size_t save_bytes = (step ? 4 : 5) * ne * sizeof(float);
   const int K = c.hist_win, nwin = (c.nt + K - 1) / K;
-  float* const st_a = c.px;  // the slot's state [5][ne]
-  auto use_state = [&](float* s5) {
-    c.px = s5; c.pz = s5 + ne; c.vx = s5 + 2 * ne; c.vz = s5 + 3 * ne; c.p = s5 + 4 * ne;
+  float* const st_a = c.state;  // the slot's state block
+  auto use_state = [&](float* s9, int par) {
+    c.set_state(s9, ne);
+    c.par = par;
   };
+  auto cur_fields = [&]() { return (step && c.par) ? c.px2 : c.px; };
   struct Restore {  // the ShotCtx points at stage A's state again on every exit
     std::function<void()> f;
     ~Restore() { f(); }
-  } restore{[&] { use_state(st_a); }};
+  } restore{[&] { use_state(st_a, 0); }};
   auto window = [&](int w) { return Window{w * K, std::min(K, c.nt - w * K)}; };
   auto stage_a = [&](int w) {
     const Window win = window(w);
@@ -799,26 +943,27 @@ void shot_operator_windowed(daw_handle* h, Batch& b, bool esource) {
   zero_state(h, c);
   for (int w = 0; w < nwin; ++w) {
     if (w > 0)
-      CK(cudaMemcpyAsync(c.ckpt + (size_t)(w - 1) * 5 * ne, st_a, state_bytes,
+      CK(cudaMemcpyAsync(c.ckpt + (size_t)(w - 1) * 5 * ne, cur_fields(), save_bytes,
                          cudaMemcpyDeviceToDevice, h->st));
     stage_a(w);
   }
   const int mode = esource ? FM_STAGE_B_ES : FM_STAGE_B;
-  use_state(c.st_b);
+  use_state(c.st_b, 0);
   zero_state(h, c);
   CK(cudaMemsetAsync(c.op_out, 0, (size_t)c.nt * c.nr * sizeof(float), h->st));
   if (esource && h->ndatum)
     CK(cudaMemsetAsync(c.d_redE, 0, (size_t)c.nt * h->ndatum * sizeof(float), h->st));
   for (int w = nwin - 1; w >= 0; --w) {
     if (w < nwin - 1) {
-      use_state(st_a);
+      const int par_b = c.par;
+      use_state(st_a, 0);
       if (w == 0)
         zero_state(h, c);
-      else
-        CK(cudaMemcpyAsync(st_a, c.ckpt + (size_t)(w - 1) * 5 * ne, state_bytes,
+      else  // into set 0, which the restarted run starts from
+        CK(cudaMemcpyAsync(c.px, c.ckpt + (size_t)(w - 1) * 5 * ne, save_bytes,
                            cudaMemcpyDeviceToDevice, h->st));
       stage_a(w);
-      use_state(c.st_b);
+      use_state(c.st_b, par_b);
     }
     const Window win = window(w);
     if (esource && c.d_cost)
@@ -1140,12 +1285,13 @@ void run_filter(daw_handle* h, const float* d_in, float* d_out, int nt, int nr, 
 // stage B's own state take the place of the rest of the history.
 size_t shot_bytes(const daw_handle* h, int nt, int nr, bool fp16, bool want_wf, int win = 0) {
   const Grid& g = h->g;
-  const size_t state = 5 * g.ext_elems() * 4;
+  const size_t state = (size_t)kStateFields * g.ext_elems() * 4;
+  const size_t saved = (size_t)5 * g.ext_elems() * 4;
   const int hs = (win > 0 && win < nt) ? win : nt;
   size_t b = state;                                        // state
   b += hist_bytes_per_step(h, fp16) * (size_t)hs;          // history (window)
   b += (size_t)(hs + 1) * 3 * kAmaxSlots * 4;
-  if (hs < nt) b += state * (size_t)((nt + hs - 1) / hs);  // saved states + stage-B state
+  if (hs < nt) b += state + saved * (size_t)((nt + hs - 1) / hs - 1);  // stage-B state + saved states
   b += (size_t)(8 + 7) * nt * nr * 4;                      // MINRES + data arrays
   b += (size_t)6 * nt * std::max(h->ndatum, 1) * 4;        // datum gathers
   if (want_wf) b += g.int_elems() * (size_t)nt * 4;
@@ -1200,7 +1346,8 @@ void prepare_shot(daw_handle* h, ShotCtx& c, const daw_shot_desc& d, int slot, b
 // Device bytes of one forward-only shot (state, one history step, data, maps).
 size_t shot_bytes_forward(const daw_handle* h, int nt, int nr) {
   const Grid& g = h->g;
-  size_t b = 5 * g.ext_elems() * 4 + hist_bytes_per_step(h, true) * 2 + 2 * 3 * kAmaxSlots * 4;
+  size_t b = (size_t)kStateFields * g.ext_elems() * 4 + hist_bytes_per_step(h, true) * 2 +
+             2 * 3 * kAmaxSlots * 4;
   b += ((size_t)8 * nt * nr + (size_t)5 * nt * std::max(h->ndatum, 1) + nt) * 4;
   b += (size_t)nr * kTile * 12 * 2 + (size_t)g.n2e * 16 * 2;
   return b;
@@ -1542,11 +1689,18 @@ int daw_create(daw_handle** out, int32_t device) {
     return DAW_ERR_CUDA;
   }
   tma_prepare(&h->persist_p, &h->persist_v, h->persist_v_mode);
+  step_prepare();
+  cudaDeviceGetAttribute(&h->sms, cudaDevAttrMultiProcessorCount, device);
+  for (int mode = 0; mode < 4; ++mode)
+    for (int f = 0; f < 2; ++f)
+      for (int t = 0; t < 2; ++t) h->step_occ[mode][f][t] = step_occupancy(mode, f != 0, t ? 32 : 16);
+  cudaGetLastError();
   // The device set-up of daw_filmartin2d_noalloc, while memory is still free
   // (not fatal here: a failure is reported again by that entry point).
   if (filter_noalloc_prepare(nullptr, 0) != DAW_OK) cudaGetLastError();
   if (cudaMalloc(&h->d_err, sizeof(unsigned)) != cudaSuccess ||
-      cudaMemset(h->d_err, 0, sizeof(unsigned)) != cudaSuccess || cudaGetLastError() != cudaSuccess) {
+      cudaMemset(h->d_err, 0, sizeof(unsigned)) != cudaSuccess ||
+      cudaMalloc(&h->d_qctr, sizeof(unsigned)) != cudaSuccess || cudaGetLastError() != cudaSuccess) {
     cudaGetLastError();
     cudaStreamDestroy(h->st);
     delete h;
@@ -1566,6 +1720,7 @@ void daw_destroy(daw_handle* h) {
   if (h->ev0) cudaEventDestroy(h->ev0);
   if (h->ev1) cudaEventDestroy(h->ev1);
   if (h->d_err) cudaFree(h->d_err);
+  if (h->d_qctr) cudaFree(h->d_qctr);
   cudaStreamDestroy(h->st);
   delete h;
 }
@@ -1599,6 +1754,16 @@ int daw_set_option(daw_handle* h, int32_t key, double value) {
         if (v < 0) throw DawError{DAW_ERR_ARG, "history window must be >= 0 (0 = automatic)"};
         h->opt.checkpoint = v;
         break;
+      case DAW_OPT_STEP_KERNEL: h->opt.step = v ? 1 : 0; break;
+      case DAW_OPT_TILE_COLS:
+        if (v != 0 && v != 16 && v != 32)
+          throw DawError{DAW_ERR_ARG, "tile columns must be 16 or 32 (0 = autotuned)"};
+        h->opt.tile_cols = v;
+        break;
+      case DAW_OPT_CTAS_PER_SM:
+        if (v < 0 || v > 3) throw DawError{DAW_ERR_ARG, "CTAs per SM must be 0..3 (0 = autotuned)"};
+        h->opt.ctas_per_sm = v;
+        break;
       default: throw DawError{DAW_ERR_ARG, "unknown option"};
     }
     if (!h->opt.fused && h->opt.history_fp16)
@@ -1620,6 +1785,9 @@ int daw_get_option(const daw_handle* h, int32_t key, double* value) {
     case DAW_OPT_MAX_BATCH: *value = o.max_batch; break;
     case DAW_OPT_CHUNK: *value = o.chunk; break;
     case DAW_OPT_CHECKPOINT: *value = o.checkpoint; break;
+    case DAW_OPT_STEP_KERNEL: *value = o.step; break;
+    case DAW_OPT_TILE_COLS: *value = o.tile_cols; break;
+    case DAW_OPT_CTAS_PER_SM: *value = o.ctas_per_sm; break;
     default: return DAW_ERR_ARG;
   }
   return DAW_OK;

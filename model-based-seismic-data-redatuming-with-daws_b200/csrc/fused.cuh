@@ -29,6 +29,9 @@ constexpr unsigned kErrNonFinite = 2u;  // NaN or Inf in a stage-A history field
 
 struct ShotDevice {
   float *px, *pz, *vx, *vz, *p;  // extended-grid state [n2e][ld]
+  // The one-kernel-per-step path (stencil_step.cu) alternates between two
+  // state sets: {px, pz, vx, vz} above and {px2, pz2, vx2, vz2}.
+  float *px2, *pz2, *vx2, *vz2;
   void* hist;                    // [nt][3][n2][n1h] (float or __half)
   unsigned* amax;                // [nt][3][kAmaxSlots] max-|x| bit patterns
   const float* amp;              // wavelet (forward) or res(nt,nr) (stage A)
@@ -53,6 +56,15 @@ struct alignas(64) TmaMaps {
   CUtensorMap vx19, vz72, px, pz, p72, vx16, vz16, kap, hist;
 };
 
+// Tensor maps of one shot for the one-kernel-per-step path (box sizes in
+// stencil_step.cu, which depend on the tile width): the four state fields of
+// both state sets and kappa with the halo of a fused pressure + velocity
+// update, and the history boxes of stage B (pressure with its halo, the
+// velocities on the tile).
+struct alignas(64) StepMaps {
+  CUtensorMap vx[2], vz[2], px[2], pz[2], kap, histp, histv;
+};
+
 struct FusedLaunch {
   const ShotDevice* shots;  // device array
   int nshots;
@@ -71,6 +83,12 @@ struct FusedLaunch {
   // max-|x| slots, the injection amplitudes in step-major order
   // [step][station] (the wavelet, or the transposed residual in stage A), the
   // record length and the station count of the injection.
+  // One-kernel-per-step path: its tensor maps, the tile queue counter (zeroed
+  // at the start of each run), the first step of the run, the state set the
+  // run starts from, the tile width and the gather units per shot.
+  const StepMaps* smaps;
+  unsigned* qctr;
+  int first, par0, tile_cols, ngath;
   static constexpr int kParamShots = 8;
   int nparam;
   const unsigned* shot_amax[kParamShots];
@@ -103,5 +121,25 @@ void fused_p_step(const Grid& g, const ModelDev& m, const FusedLaunch& L, int mo
 void fused_v_step(const Grid& g, const ModelDev& m, const FusedLaunch& L, int mode, int it,
                   cudaStream_t st);
 int fused_warps(const Grid& g, int chunk);
+
+// One kernel per time step (stencil_step.cu): the pressure update of step it,
+// recomputed on the velocity stencil's halo, then the velocity update, from
+// state set (par0 + it - first) & 1 into the other set; plus, for step it - 1,
+// the stage-A history stores and the receiver / datum gathers.  Steps run
+// first .. last + 1, the extra launch doing only the work of the last step.
+// Tile widths: 16 or 32 columns.
+struct StepConfig {
+  int tile_cols = 32;  // 16 or 32
+  int ctas_per_sm = 0; // 0 = as many as fit
+};
+// Dynamic shared memory and resident CTAs per SM of the instantiation
+// (mode, fp16, tile width); call once per device outside graph capture.
+void step_prepare();
+int step_occupancy(int mode, bool fp16, int tile_cols);
+int step_tiles(const Grid& g, int tile_cols);
+void step_launch(const Grid& g, const ModelDev& m, const FusedLaunch& L, int mode, int it,
+                 int grid, cudaStream_t st);
+bool step_encode_maps(const Grid& g, float* const st[2][4], const float* kap, const void* hist,
+                      int hist_fp16, int n1h, int nsteps, int tile_cols, StepMaps* out);
 
 }  // namespace daw

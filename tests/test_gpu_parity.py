@@ -36,7 +36,13 @@ def handle(pkg, case, preset="plain", **opt):
     return h
 
 
+# "mixed" with FP32 histories: the one-kernel-per-step TMA path (autotuned
+# tile width, and both widths pinned), the split pressure/velocity TMA kernels
+# (step 0), direct launches instead of graphs, and the register kernels.
 PATHS = [("plain", {}), ("mixed", {"history": 0}), ("mixed", {"history": 0, "graph": 0}),
+         ("mixed", {"history": 0, "tile_cols": 16, "ctas_per_sm": 1}),
+         ("mixed", {"history": 0, "tile_cols": 32, "ctas_per_sm": 2}),
+         ("mixed", {"history": 0, "step": 0}),
          ("mixed", {"history": 0, "chunk": 1}), ("mixed", {"history": 0, "chunk": 4})]
 
 
