@@ -80,8 +80,9 @@ enum daw_option {
                                 0 = separate pressure and velocity kernels */
   DAW_OPT_TILE_COLS = 10,    /* one-kernel-per-step tiles: 16 or 32 columns of 64
                                 rows; 0 (default) = chosen by the autotuner */
-  DAW_OPT_CTAS_PER_SM = 11   /* one-kernel-per-step CTAs per SM (1..3, bounded by
-                                occupancy); 0 (default) = chosen by the autotuner */
+  DAW_OPT_CTAS_PER_SM = 11   /* one-kernel-per-step CTAs per SM (1..3; a value above
+                                what fits is lowered to the occupancy); 0 (default) =
+                                chosen by the autotuner */
 };
 
 /* Handle lifetime ------------------------------------------------------- */

@@ -715,9 +715,11 @@ daw_handle::Tuned tune_step(daw_handle* h, Batch& b, int mode, FusedLaunch L, in
   std::vector<daw_handle::Tuned> cands;
   for (int tc : {16, 32}) {
     if (h->opt.tile_cols && h->opt.tile_cols != tc) continue;
-    const int occ = h->step_occ[tmode][f][tc == 32 ? 1 : 0];
-    for (int c = 1; c <= std::min(occ, 3); ++c)
-      if (!h->opt.ctas_per_sm || h->opt.ctas_per_sm == c) cands.push_back({tc, c, 0.f});
+    // a pinned CTA count above what fits is clamped to the occupancy
+    const int occ = std::min(h->step_occ[tmode][f][tc == 32 ? 1 : 0], 3);
+    const int pin = h->opt.ctas_per_sm ? std::min(h->opt.ctas_per_sm, occ) : 0;
+    for (int c = 1; c <= occ; ++c)
+      if (!pin || pin == c) cands.push_back({tc, c, 0.f});
   }
   if (cands.empty())
     throw DawError{DAW_ERR_CUDA, "no resident configuration of the step kernel"};
