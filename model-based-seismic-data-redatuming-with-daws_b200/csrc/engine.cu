@@ -812,6 +812,7 @@ void run_fused(daw_handle* h, Batch& b, int mode, const Window* w = nullptr) {
     }
     L.par0 = std::max(par0, 0);
     L.first = first;
+    L.step_last = nt_v;
     L.qctr = h->d_qctr;
     L.ngath = mode == FM_STAGE_A ? 0 : (L.max_rec + (b.no_datum ? 0 : L.max_datum) + 7) / 8;
     const daw_handle::Tuned t = tune_step(h, b, mode, L, first);

@@ -89,6 +89,7 @@ struct FusedLaunch {
   const StepMaps* smaps;
   unsigned* qctr;
   int first, par0, tile_cols, ngath;
+  int step_last;  // last stencil step of the run (the extra launch after it does none)
   static constexpr int kParamShots = 8;
   int nparam;
   const unsigned* shot_amax[kParamShots];

@@ -128,7 +128,7 @@ struct ShotStep {
 template <int MODE>
 __device__ __forceinline__ ShotStep shot_step(const FusedLaunch& L, int nt, bool active, int it) {
   ShotStep s;
-  s.step = active && it <= nt;
+  s.step = active && it <= nt && it <= L.step_last;
   s.defer = active && it > L.first && it - 1 <= nt;
   return s;
 }
@@ -263,7 +263,7 @@ __global__ void __launch_bounds__(kT, 2)
     const StepMaps* mp = L.smaps + id.shot;
     unsigned char* st = smem + s * kStage;
     const int nt = shot_nt(L, id.shot);
-    const bool hist = kB && it <= nt;
+    const bool hist = kB && it <= nt && it <= L.step_last;
     bar_expect(&bar[s], G::tx(hist, FP16));
     tma_2d(st, &mp->vx[pin], id.r0 - SH, id.c0 - 3, &bar[s]);
     tma_2d(st + G::kVX, &mp->vz[pin], id.r0 - SH, id.c0 - 1, &bar[s]);
