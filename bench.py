@@ -1,28 +1,41 @@
-"""Benchmark: shots/hour of DAW redatuming on the 751x2301 (h = 4 m) model.
+"""Benchmark: shots/hour of batched mixed-precision DAW redatuming on the
+751x2301 (h = 4 m) model.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--config 4|2] [--batch B] [--checkpoint K] [--nt NT --maxiter M]
 
-Workload (one step = one batch of shots through the whole hot path): the
-751x2301 model, npml 40, nt = 7500 at dt = 0.4 ms, 576 receivers every 16 m,
-15 Hz Ricker, 20 MINRES iterations, datum receivers at 1200 m; every shot is
-forward modelling, the MINRES solve of the data-assimilation normal equation
-(2 + 1 + 20 G G^T applications), the final extended-source simulation, the
-on-the-fly datum extraction and the band-pass filter.  Inputs are seeded
-synthetic data of those shapes (the reference publishes no data set).
+Workload (--config 4, the default: the metric's own configuration): the
+751x2301 model, npml 40, dt = 0.4 ms, 15 Hz Ricker, 20 MINRES iterations,
+datum receivers every 16 m at 1200 m, and the seeded 256-shot set with record
+lengths nt ~ U[3000, 7500] and receiver spreads of 100-576 channels (split
+offsets).  Mixed precision: FP32 stencils, FP16 wavefield histories with one
+power-of-two scale per shot, step and field, FP64 MINRES scalars.  One step =
+the next batch of this rank's shots, as many as HBM admits (each shot's own
+nt and spread), through the whole hot path: forward modelling, the MINRES
+solve (2 + 1 + 20 G G^T applications), the final extended-source simulation,
+the on-the-fly datum extraction and the band-pass filter.  --config 2 runs
+the uniform 50-shot variant instead (nt 7500, 576 receivers, batches of
+--batch shots).  Inputs are seeded synthetic data of those shapes (the
+reference publishes no data set); observed data are modelled in the true
+model on the GPU before timing.  Density is 1 as in the reference
+(src/submodeling2.f90:93).
 
-`value`: mixed path (FP32 stencils, FP16 histories with per-step power-of-two
-scales, FP64 MINRES scalars), shots batched per launch, inputs resident in
-HBM.  `e2e`: the same through daw_shots with host buffers.  `plain_fp32`: the
-plain FP32 GPU port (kernel per reference loop, FP32 histories) on one shot of
-the same workload.  The reference arm (--impl reference) times the CPU
-restatement of the reference (FP32, one single-threaded process per core as
-the reference's MPI ranks run) on a truncated sample scaled by point updates.
+`value`: device time of the batches with their inputs staged in HBM (the
+stage-in is untimed).  `e2e`: the same shots through daw_shots with host
+buffers, host-device copies included.  Denominators on the first timed
+batch's shots: `plain_fp32` (kernel per reference loop, FP32 histories and
+scalars) and `fused_fp32` (the same one-kernel-per-step kernels with FP32
+histories and FP32 scalars).  `accuracy`: the mixed path against the FP64
+oracle on the whole 151x461 single-shot configuration, and against the
+FP32-history kernels on the timed batch.  The reference arm (--impl
+reference) times the CPU restatement of the reference (FP32, one
+single-threaded process per core as the reference's MPI ranks run) on a
+truncated sample scaled by point updates.
 """
 from __future__ import annotations
 
 import argparse
 import json
-import math
 import multiprocessing as mp
 import os
 import signal
@@ -30,6 +43,7 @@ import statistics
 import subprocess
 import sys
 import tempfile
+import threading
 import time
 
 import numpy as np
@@ -39,9 +53,9 @@ sys.path.insert(0, ROOT)
 import __graft_entry__ as entry  # noqa: E402
 
 PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
-# DRAM bytes of one G G^T time step (p + v kernels), measured by ncu on the
-# same grid and batch
-TRAFFIC = os.path.join(ROOT, "profiles", "k_tma_751x2301_traffic.json")
+# DRAM bytes per shot time step of the step kernels, measured by ncu on the
+# same grid
+TRAFFIC = os.path.join(ROOT, "profiles", "k_step_751x2301_traffic.json")
 METRIC = "shots/hour redatumed at <=1e-3 rel err vs FP64: batched mixed vs plain FP32"
 
 
@@ -49,36 +63,77 @@ def env_int(k, d):
     return int(os.environ.get(k, d))
 
 
+def rel(a, b):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    d = np.linalg.norm(b)
+    return float(np.linalg.norm(a - b) / (d if d > 0 else 1.0))
+
+
 # ---------------------------------------------------------------------------
-# workload
+# workloads
 # ---------------------------------------------------------------------------
-def make_workload(nt=None):
+def make_workload(config=4, nt=None):
     entry.load_package()
     from daw_b200 import synthetic
-    w = synthetic.config2(2, nshot=50, nt=nt or 7500)
+    if config == 4:
+        w = synthetic.config3(3, nshot=256)
+        w.name = "cfg4"
+    else:
+        w = synthetic.config2(2, nshot=50, nt=nt or 7500)
     return w
 
 
-def shot_dicts(pkg, h, w, shot_ids, model_dobs=True):
-    """Observed data are modelled in the true model (mode 0) on the GPU.  The
-    reduced profiling variants use dobs = 0 instead: their records are too
-    short for a reflection to separate the true and background models, and a
-    zero residual would stop MINRES before its first iteration."""
-    rec = pkg.subacqui(w.rec_pos[0], w.h, w.npml, w.ofs)
-    s = w.wavelet(w.nt)
-    h.set_model(w.vtrue, w.npml, w.h, w.dt, w.ofs)
+def workload_text(w, args):
+    if w.name == "cfg4":
+        return ("751x2301 h=4 m, npml 40, 256 shots with nt U[3000,7500] @ 0.4 ms and 100-576 "
+                "receivers (seeded split offsets), 15 Hz, 20 MINRES iterations, datum at 1200 m, "
+                "FP16 histories / FP64 MINRES scalars")
+    txt = (f"751x2301 h=4 m, npml 40, nt {w.nt} @ 0.4 ms, 576 receivers, 15 Hz, {w.maxiter} MINRES "
+           f"iterations, datum at 1200 m")
+    if w.nt != 7500 or w.maxiter != 20:
+        txt += " (reduced profiling variant with dobs = 0, not the benchmark)"
+    return txt
+
+
+def shot_dicts(pkg, h, w, ids, model_dobs=True):
+    """The shots `ids` of the workload; observed data modelled in the true
+    model (mode 0, batched) on the GPU.  Reduced profiling variants use dobs =
+    0: their records are too short for a reflection to separate the models,
+    and a zero residual would stop MINRES at once, so it is not used there."""
     shots = []
-    for i in shot_ids:
+    for i in ids:
+        nt = w.nts[i]
+        rec = pkg.subacqui(w.rec_pos[i], w.h, w.npml, w.ofs)
         src = pkg.subacqui(w.src_pos[i:i + 1], w.h, w.npml, w.ofs)[0]
-        if model_dobs:
-            dobs, _ = h.submodeling(s, src, rec)
-        else:
-            dobs = np.zeros((w.nt, rec.shape[0]), np.float32, order="F")
-        shots.append(dict(s=s, nt=w.nt, src=src, rec=rec, dobs=dobs, mu=w.mu,
-                          maxiter=w.maxiter, rtol=0.0, band=w.band, shot=i + 1))
+        shots.append(dict(s=w.wavelet(nt), nt=nt, src=src, rec=rec, mu=w.mu, maxiter=w.maxiter,
+                          rtol=0.0, band=w.band, shot=i + 1))
+    if model_dobs:
+        h.set_model(w.vtrue, w.npml, w.h, w.dt, w.ofs)
+        data = h.submodeling_shots(shots)
+        for sh, d in zip(shots, data):
+            sh["dobs"] = d
+    else:
+        for sh in shots:
+            sh["dobs"] = np.zeros((sh["nt"], sh["rec"].shape[0]), np.float32, order="F")
     h.set_model(w.c0, w.npml, w.h, w.dt, w.ofs)
     h.set_datum(pkg.subacqui(w.datum_pos, w.h, w.npml, w.ofs))
     return shots
+
+
+def stage_batch(pkg, h, shots, start, cap):
+    """Stages the longest run of shots from `start` (at most `cap`) that HBM
+    admits as one batch; returns its length."""
+    k = min(cap, len(shots) - start)
+    while k >= 1:
+        try:
+            h.stage_shots(shots[start:start + k])
+            return k
+        except pkg.DawError as e:
+            if e.code != -2 or k == 1:
+                raise
+            k -= 1
+    raise RuntimeError("no shot admitted")
 
 
 # ---------------------------------------------------------------------------
@@ -143,33 +198,36 @@ SAMPLE_NT = 100
 def _cpu_worker(args):
     import __graft_entry__ as e
     O = e.load_oracle()
-    w = make_workload()
-    from daw_b200 import synthetic  # noqa
+    sample_nt, shot = args
+    w = make_workload(2)
     rec = O.acqui_table(w.rec_pos[0], w.h, w.npml, w.ofs)
-    src = O.acqui_table(w.src_pos[args:args + 1], w.h, w.npml, w.ofs)[0]
-    nt = SAMPLE_NT
-    s = w.wavelet(w.nt)[:nt]
-    dobs = np.zeros((nt, rec.shape[0]), np.float32, order="F")
+    src = O.acqui_table(w.src_pos[shot:shot + 1], w.h, w.npml, w.ofs)[0]
+    s = w.wavelet(w.nt)[:sample_nt]
+    dobs = np.zeros((sample_nt, rec.shape[0]), np.float32, order="F")
     t0 = time.perf_counter()
-    upd = O.baseline_sample(w.c0, w.npml, w.h, w.ofs, nt, w.dt, s, src, rec, dobs, w.mu, 1)
+    upd = O.baseline_sample(w.c0, w.npml, w.h, w.ofs, sample_nt, w.dt, s, src, rec, dobs, w.mu, 1)
     return time.perf_counter() - t0, upd
 
 
-def cpu_baseline(max_procs=None):
-    w = make_workload()
+def cpu_baseline(w, max_procs=None, sample_nt=SAMPLE_NT):
+    """The FP32 CPU restatement on every host core (one single-threaded
+    process per core), each process one 751x2301 shot truncated to sample_nt
+    steps and one MINRES iteration; scaled by point updates to the workload's
+    mean shot."""
     ne = (w.n1 + 2 * w.npml) * (w.n2 + 2 * w.npml)
-    full = (7 + 2 * w.maxiter) * w.nt * ne  # point updates of one full shot
+    mean_nt = float(np.mean(w.nts))
+    full = (7 + 2 * w.maxiter) * mean_nt * ne  # point updates of the mean shot
     ncpu = os.cpu_count() or 1
     try:
         avail = os.sysconf("SC_AVPHYS_PAGES") * os.sysconf("SC_PAGE_SIZE")
     except (ValueError, OSError):
         avail = 16 << 30
-    per_proc = 3 * w.n1 * w.n2 * SAMPLE_NT * 4 + 12 * ne * 4 + (256 << 20)
+    per_proc = 3 * w.n1 * w.n2 * sample_nt * 4 + 12 * ne * 4 + (256 << 20)
     procs = max(1, min(ncpu, int(avail * 0.6 // per_proc), max_procs or ncpu))
     ctx = mp.get_context("spawn")
     t0 = time.perf_counter()
     with ctx.Pool(procs) as pool:
-        res = pool.map(_cpu_worker, [i % 50 for i in range(procs)])
+        res = pool.map(_cpu_worker, [(sample_nt, i % 50) for i in range(procs)])
     wall = time.perf_counter() - t0
     t_sample = max(r[0] for r in res)
     upd = res[0][1]
@@ -177,18 +235,62 @@ def cpu_baseline(max_procs=None):
     value = procs * 3600.0 / t_shot
     return dict(value=value, unit="shots/hour", cores=procs, kind="port",
                 sample=(f"{procs} single-threaded processes (one per core), each one 751x2301 "
-                        f"shot truncated to nt={SAMPLE_NT} with 1 MINRES iteration "
+                        f"shot truncated to nt={sample_nt} with 1 MINRES iteration "
                         f"({upd:.3g} point updates, {t_sample:.1f} s), scaled by point updates "
-                        f"to the full shot ({full:.3g}); FP32 CPU restatement of the reference"),
-                wall_s=wall)
+                        f"to the workload's mean shot ({full:.3g}); FP32 CPU restatement of the "
+                        f"reference"),
+                wall_s=wall, ns_per_update=t_sample / upd * 1e9)
+
+
+class Cfg1Oracle:
+    """The whole 151x461 single-shot configuration (nt 2000, 10 MINRES
+    iterations) on the CPU oracle in background threads (ctypes releases the
+    GIL): in FP64 as the accuracy reference of the mixed path, and in FP32
+    timed, a full CPU shot that checks the point-update scaling of the CPU
+    baseline's truncated samples."""
+
+    def __init__(self, pkg):
+        self.O = entry.load_oracle()
+        from daw_b200 import synthetic
+        w = synthetic.config1()
+        self.w = w
+        self.src = pkg.subacqui(w.src_pos, w.h, w.npml, w.ofs)[0]
+        self.rec = pkg.subacqui(w.rec_pos[0], w.h, w.npml, w.ofs)
+        self.ird = pkg.subacqui(w.datum_pos, w.h, w.npml, w.ofs)
+        self.s = w.wavelet()
+        self.dobs, _ = self.O.submodeling(w.vtrue, w.npml, w.h, w.ofs, w.nt, w.dt, self.s,
+                                          self.src, self.rec)
+        self.res = {}
+        self.threads = [threading.Thread(target=self._run, args=(p,)) for p in ("f64", "f32")]
+        for t in self.threads:
+            t.start()
+
+    def _run(self, prec):
+        w = self.w
+        t0 = time.perf_counter()
+        out = self.O.daw_shot(w.c0, w.npml, w.h, w.ofs, w.nt, w.dt, self.s, self.src, self.rec,
+                              self.dobs, w.mu, w.maxiter, 0.0, self.ird, w.band, prec=prec)
+        self.res[prec] = (out, time.perf_counter() - t0)
+
+    def gpu_shot(self, pkg, local):
+        w = self.w
+        with pkg.Handle(local, preset="mixed") as h:
+            h.set_model(w.c0, w.npml, w.h, w.dt, w.ofs)
+            h.set_datum(self.ird)
+            return h.shot(s=self.s, nt=w.nt, src=self.src, rec=self.rec, dobs=self.dobs, mu=w.mu,
+                          maxiter=w.maxiter, rtol=0.0, band=w.band)
+
+    def join(self):
+        for t in self.threads:
+            t.join()
 
 
 # ---------------------------------------------------------------------------
 def op_steps_per_application(nt, window):
-    """Time steps of one G G^T application: stage A (nt steps + the history
-    flush step) and stage B (nt steps); with history windows of `window`
-    steps, stage A also re-runs every window but the last, each with its own
-    flush step."""
+    """Time steps of one G G^T application with the split kernels: stage A
+    (nt steps + the history flush step) and stage B (nt steps); with history
+    windows of `window` steps, stage A also re-runs every window but the last,
+    each with its own flush step."""
     if window <= 0 or window >= nt:
         return 2 * nt + 1
     nwin = -(-nt // window)
@@ -196,30 +298,59 @@ def op_steps_per_application(nt, window):
     return nt + (nt - last) + (2 * nwin - 1) + nt
 
 
-def roofline(pkg, tim, nshots, w, steps_per_op):
+def roofline(tim, w, fp16=True):
+    """The step kernels of the G G^T stages (stage A and stage B, one launch
+    per time step): algorithmic bytes per shot step = 36 B per extended point
+    (px, pz, vx, vz read and written, kappa read) + 3 history fields per
+    interior point (written in stage A, read in stage B: 2 B each in FP16),
+    over the device time of those time loops."""
     peaks = json.load(open(PEAKS)) if os.path.exists(PEAKS) else {}
     peak = peaks.get("hbm_gbs", 6650.0)
     ne = (w.n1 + 2 * w.npml) * (w.n2 + 2 * w.npml)
     ni = w.n1 * w.n2
-    # dominant work: one fused time step (pressure + velocity kernel) of the
-    # G G^T stages; algorithmic bytes per shot-step: 36 B per extended point
-    # (px,pz,vx,vz read+write, kappa read) + 6 B per interior point (three FP16
-    # history fields written in stage A / read in stage B)
-    per_step = (36.0 * ne + 6.0 * ni) * nshots
-    ms = tim["operator_ms"]
-    launches = steps_per_op
+    per_shot_step = 36.0 * ne + 3 * (2 if fp16 else 4) * ni
+    shot_steps = tim["shot_steps_a"] + tim["shot_steps_b"]
+    ms = tim["sim_a_ms"] + tim["sim_b_ms"]
+    launches = tim["steps_a"] + tim["steps_b"]
+    achieved = per_shot_step * shot_steps / (ms * 1e-3) / 1e9
     avg_ms = ms / max(launches, 1)
-    achieved = per_step / (avg_ms * 1e-3) / 1e9
-    traffic, traffic_note = None, None
+    bytes_per_launch = per_shot_step * shot_steps / max(launches, 1)
+    traffic, note = None, None
     if os.path.exists(TRAFFIC):
         t = json.load(open(TRAFFIC))
-        traffic = t["step_bytes"] * nshots / t["shots_per_launch"]
-        traffic_note = t["note"]
+        traffic = t["bytes_per_shot_step"] * shot_steps / max(launches, 1)
+        note = t["note"]
     return {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-            "frac": achieved / peak, "traffic": traffic, "traffic_note": traffic_note,
+            "frac": achieved / peak, "traffic": traffic, "traffic_note": note,
             "peak_source": "measured" if peaks else "fallback",
-            "unit_of_work": "one fused time step (p+v kernels) of the G G^T stages",
-            "bytes_per_step": per_step, "avg_step_ms": avg_ms}
+            "unit_of_work": "one launch of the step kernel (one time step of every shot of the "
+                            "batch) in the G G^T stages",
+            "bytes_per_launch": bytes_per_launch, "avg_launch_ms": avg_ms,
+            "bytes_per_shot_step": per_shot_step}
+
+
+def reference_runs(pkg, local, shots, base_out):
+    """The plain FP32 port and the FP32-history step kernels on `shots`, one
+    staged batch at a time; shots/hour of each and the mixed path's error
+    against the FP32-history outputs."""
+    res = {}
+    for name, preset, opt in (("plain_fp32", "plain", {}),
+                              ("fused_fp32", "mixed", {"history": 0, "scalars": 0})):
+        with pkg.Handle(local, preset=preset, **opt) as h:
+            h.set_model(*base_out["model"])
+            h.set_datum(base_out["datum"])
+            ms, outs, launches, i = 0.0, [], 0, 0
+            while i < len(shots):
+                k = stage_batch(pkg, h, shots, i, len(shots))
+                h.reset_timing()
+                ms += h.run_staged()
+                launches += h.timing()["kernel_launches"]
+                outs += h.fetch_staged(outputs=("deltade", "redatumed"))
+                i += k
+            res[name] = {"value": len(shots) * 3600.0 / (ms * 1e-3), "unit": "shots/hour",
+                         "ms": ms, "shots": len(shots), "kernel_launches": int(launches),
+                         "outs": outs}
+    return res
 
 
 def run_ours(args):
@@ -227,98 +358,172 @@ def run_ours(args):
     from daw_b200 import ranks
     rank, world, local = ranks.rank_env()
     dist = ranks.init_group(world)
-    w = make_workload(args.nt)
+    w = make_workload(args.config, args.nt)
     if args.maxiter is not None:
         w.maxiter = args.maxiter
-    B = args.batch
-    # this rank's shots: the first B of its para_range block of the 50 shots
-    ids = ranks.rank_shots(len(w.src_pos), B, rank, world)
-    reduced = w.nt != 7500 or w.maxiter != 20  # profiling-sized variant
-    h = pkg.Handle(local, preset="mixed", checkpoint=args.checkpoint)
+    reduced = args.config == 2 and (w.nt != 7500 or w.maxiter != 20)
+    cfg1 = None
+    if rank == 0 and world == 1 and not reduced and not args.no_accuracy:
+        cfg1 = Cfg1Oracle(pkg)  # CPU threads overlap the GPU timing
+    # this rank's shots (para_range of the shot set), cycled when a run needs more
+    nsh = len(w.src_pos)
+    ista, iend = ranks.para_range(1, nsh, world, rank)
+    mine = list(range(ista - 1, iend))
+    cap = args.batch if args.config == 2 else 8
+    h = pkg.Handle(local, preset="mixed", checkpoint=args.checkpoint,
+                   step=1 if args.kernel == "step" else 0)
+    if args.config == 2:
+        per_step = args.batch
+        need = per_step
+    else:
+        need = min(len(mine), 4 * (args.warmup + args.steps))
+    ids = [mine[i % len(mine)] for i in range(need)]
     shots = shot_dicts(pkg, h, w, ids, model_dobs=not reduced)
-    h.stage_shots(shots)
-    for _ in range(args.warmup):
-        h.run_staged()
+    # steps: consecutive admitted batches (config 2: the same batch each step)
+    pos = 0
+    dev_ms, step_shots = [], []
+    first_batch = None
 
+    def one_step(timed):
+        nonlocal pos, first_batch
+        if args.config == 2:
+            if pos == 0:
+                stage_batch(pkg, h, shots, 0, cap)
+                pos = 1
+            k = len(shots)
+        else:
+            if pos >= len(shots):
+                pos = 0
+            k = stage_batch(pkg, h, shots, pos, cap)
+            if timed and first_batch is None:
+                first_batch = shots[pos:pos + k]
+            pos += k
+        ms = h.run_staged()
+        if timed:
+            dev_ms.append(ms)
+            step_shots.append(k)
+        return k
+
+    for _ in range(args.warmup):
+        one_step(False)
+    if args.config == 2:
+        first_batch = shots
     h.reset_timing()
     ranks.barrier(dist)
-    dev_ms = []
     with Clocks(local) as clk:
         for _ in range(args.steps):
-            dev_ms.append(h.run_staged())
+            one_step(True)
     ranks.barrier(dist)
     tim = h.timing()
     total_ms = ranks.max_over_ranks(dist, sum(dev_ms))
-    shots_done = B * args.steps * world
+    shots_done = ranks.sum_over_ranks(dist, sum(step_shots))
     value = shots_done * 3600.0 / (total_ms * 1e-3)
-    # G G^T applications per shot: the shift's (1), the reference's unused one
-    # (1) and one per MINRES iteration (rtol 0: all run); each is stage A (nt
-    # steps + the history flush step) followed by stage B (nt steps)
-    op_steps = op_steps_per_application(w.nt, args.checkpoint) * (2 + w.maxiter) * args.steps
-    roof = roofline(pkg, tim, B, w, op_steps)
-    # accuracy of the mixed path against the FP32-history fused path on the same shots
-    out_mixed = h.fetch_staged(outputs=("deltade", "redatumed"))
-    # e2e through the public API with host buffers
+    roof = roofline(tim, w)
+    upd_per_s = tim["point_updates"] / (sum(dev_ms) * 1e-3) * world
+    # mixed outputs of the first timed batch (accuracy against FP32 histories)
+    mixed_first = None
+    if rank == 0 and not args.no_plain:
+        k = stage_batch(pkg, h, first_batch, 0, len(first_batch))
+        h.run_staged()
+        mixed_first = h.fetch_staged(outputs=("deltade", "redatumed"))[:k]
+        first_batch = first_batch[:k]
+    # e2e through the public API with host buffers (daw_shots forms its batches)
     e2e = None
     if not args.no_e2e:
-        h.reset_timing()
+        e2e_shots = first_batch
         t0 = time.perf_counter()
-        outs = h.shots(shots, outputs=("deltade", "redatumed"))
+        outs = h.shots(e2e_shots, outputs=("deltade", "redatumed"))
         e2e_s = time.perf_counter() - t0
-        h_bytes = sum(sh["s"].nbytes + sh["dobs"].nbytes + sh["rec"].nbytes for sh in shots)
+        h_bytes = sum(sh["s"].nbytes + sh["dobs"].nbytes + sh["rec"].nbytes for sh in e2e_shots)
         d_bytes = sum(o["deltade"].nbytes + o["redatumed"].nbytes for o in outs)
-        e2e = {"value": B * 3600.0 / e2e_s, "unit": "shots/hour",
-               "h2d_bytes_per_step": int(h_bytes), "d2h_bytes_per_step": int(d_bytes)}
+        e2e = {"value": len(e2e_shots) * 3600.0 / e2e_s * world, "unit": "shots/hour",
+               "h2d_bytes_per_step": int(h_bytes), "d2h_bytes_per_step": int(d_bytes),
+               "shots_per_step": len(e2e_shots)}
+    model = (w.c0, w.npml, w.h, w.dt, w.ofs)
+    datum = pkg.subacqui(w.datum_pos, w.h, w.npml, w.ofs)
     h.close()
     del h
-    result = None
-    plain = None
+    plain = fused = acc = None
     if rank == 0 and not args.no_plain:
-        hp = pkg.Handle(local, preset="plain")
-        hp.set_model(w.c0, w.npml, w.h, w.dt, w.ofs)
-        hp.set_datum(pkg.subacqui(w.datum_pos, w.h, w.npml, w.ofs))
-        hp.stage_shots(shots[:1])
-        hp.reset_timing()
-        pms = hp.run_staged()
-        ptim = hp.timing()
-        out_plain = hp.fetch_staged(outputs=("deltade", "redatumed"))
-        hp.close()
-        err_red = float(np.linalg.norm(out_mixed[0]["redatumed"] - out_plain[0]["redatumed"]) /
-                        np.linalg.norm(out_plain[0]["redatumed"]))
-        err_de = float(np.linalg.norm(out_mixed[0]["deltade"] - out_plain[0]["deltade"]) /
-                       np.linalg.norm(out_plain[0]["deltade"]))
-        plain = {"value": 3600.0 / (pms * 1e-3), "unit": "shots/hour", "ms_per_shot": pms,
-                 "kernel_launches": int(ptim["kernel_launches"]),
-                 "mixed_vs_plain_rel_l2": {"redatumed": err_red, "deltade": err_de},
-                 "ratio_mixed_over_plain": value / world / (3600.0 / (pms * 1e-3))}
+        refs = reference_runs(pkg, local, first_batch, {"model": model, "datum": datum})
+        out32 = refs["fused_fp32"].pop("outs")
+        outp = refs["plain_fp32"].pop("outs")
+        per_shot_value = value / world
+        plain, fused = refs["plain_fp32"], refs["fused_fp32"]
+        # the denominators ran the first timed batch's shots; the mixed path's
+        # shots/hour on the same shots comes from its device time per shot-step
+        mixed_same = None
+        if args.config == 4:
+            mixed_same = len(first_batch) * 3600.0 / (dev_ms[0] * 1e-3)
+        plain["ratio_mixed_over_plain"] = (mixed_same or per_shot_value) / plain["value"]
+        fused["ratio_mixed_over_fused_fp32"] = (mixed_same or per_shot_value) / fused["value"]
+        plain["mixed_vs_plain_rel_l2"] = {
+            "redatumed": max(rel(a["redatumed"], b["redatumed"]) for a, b in zip(mixed_first, outp)),
+            "deltade": max(rel(a["deltade"], b["deltade"]) for a, b in zip(mixed_first, outp))}
+        acc = {"batch_mixed_vs_fp32_history": {
+            "shots": [sh["shot"] for sh in first_batch],
+            "redatumed": max(rel(a["redatumed"], b["redatumed"]) for a, b in zip(mixed_first, out32)),
+            "deltade": max(rel(a["deltade"], b["deltade"]) for a, b in zip(mixed_first, out32)),
+            "note": "max over the batch's shots of rel. L2 against the same kernels with FP32 "
+                    "histories and FP32 MINRES scalars, full nt and 20 iterations"}}
     cpu = None
+    if cfg1 is not None:
+        g1 = cfg1.gpu_shot(pkg, local)
+        cfg1.join()
+        r64, t64 = cfg1.res["f64"]
+        r32, t32 = cfg1.res["f32"]
+        acc = acc or {}
+        acc["cfg1_mixed_vs_f64"] = {
+            k: rel(g1[k], r64[k]) for k in ("datar", "deltade", "dataesc", "datae",
+                                            "redatumed_raw", "redatumed")}
+        acc["cfg1_mixed_vs_f64"]["workload"] = ("151x461 h=20 m, npml 20, nt 2000, 230 receivers, "
+                                                "10 MINRES iterations, whole shot")
+        cw = cfg1.w
+        cfg1_upd = (7 + 2 * cw.maxiter) * cw.nt * (cw.n1 + 2 * cw.npml) * (cw.n2 + 2 * cw.npml)
+        cfg1_full = {"seconds": t32, "ns_per_update": t32 / cfg1_upd * 1e9,
+                     "note": "one whole 151x461 shot (nt 2000, 10 iterations) of the FP32 CPU "
+                             "restatement, one thread, timed while the GPU bench ran"}
     if rank == 0 and world == 1 and not args.no_cpu and not reduced:
         print(json.dumps({"partial": True, "value": value, "e2e": e2e, "plain_fp32": plain}),
               file=sys.stderr, flush=True)
         try:
-            cpu = cpu_baseline(args.cpu_procs)
+            cpu = cpu_baseline(w, args.cpu_procs)
+            if cfg1 is not None:
+                cpu["full_shot_check"] = cfg1_full
         except Exception as ex:  # the GPU line is still reported
             cpu = {"error": f"{type(ex).__name__}: {ex}"}
     if rank == 0:
+        tc = {m: (tim["tile_cols"][i], tim["ctas_per_sm"][i])
+              for i, m in enumerate(("forward", "stage_a", "stage_b", "esource"))}
         result = {
             "metric": METRIC, "value": value, "unit": "shots/hour", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": total_ms / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32 stencil / f16 history / f64 scalars",
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 stencil / f16 history / f64 scalars",
             "data": "synthetic (seeded; observed data modelled in the true model)",
-            "config": {"workload": f"751x2301 h=4 m, npml 40, nt {w.nt} @ 0.4 ms, 576 receivers, "
-                                   f"15 Hz, {w.maxiter} MINRES iterations, datum at 1200 m"
-                                   + (" (reduced profiling variant with dobs = 0, not the "
-                                      "benchmark)" if reduced else ""),
-                       "shots_per_step_per_gpu": B, "parallelism": f"shots x{world} (no collective)",
+            "config": {"workload": workload_text(w, args),
+                       "shots_per_step": [int(x) for x in step_shots],
+                       "shots_timed": int(shots_done),
+                       "batching": ("consecutive shots, as many as HBM admits per batch"
+                                    if args.config == 4 else f"{args.batch} shots per batch"),
+                       "density": "1 (the reference's rho = 1, src/submodeling2.f90:93)",
+                       "kernel": ("one TMA kernel per time step (p recomputed on the v halo)"
+                                  if args.kernel == "step" else
+                                  "split TMA pressure and velocity kernels"),
+                       "autotuned_tile_cols_ctas_per_sm": tc,
+                       "parallelism": f"shots x{world} (para_range, no collective)",
                        "stage_a_history": (f"windows of {args.checkpoint} steps (checkpointed)"
-                                           if 0 < args.checkpoint < w.nt else "whole record"),
-                       "l2": "working set (78 GB FP16 history per shot) far exceeds L2"},
+                                           if args.checkpoint > 0 else "whole record"),
+                       "l2": "working set (30-78 GB of FP16 history per shot) far exceeds L2"},
             "clocks": clk.summary(),
             "e2e": e2e,
             "gpu_launches": int(tim["kernel_launches"]),
+            "grid_point_updates_per_s": upd_per_s,
             "roofline": roof,
             "plain_fp32": plain,
+            "fused_fp32": fused,
+            "accuracy": acc,
             "cpu_baseline": cpu,
             "timing_ms": {k: tim[k] for k in ("forward_ms", "operator_ms", "minres_vec_ms",
                                               "esource_ms", "filter_ms")},
@@ -333,10 +538,11 @@ def run_reference(args):
     rank, world = env_int("RANK", 0), env_int("WORLD_SIZE", 1)
     if rank != 0:
         return
+    w = make_workload(args.config, args.nt)
     K, W = args.steps, args.warmup
     vals = []
     for i in range(W + K):
-        r = cpu_baseline(args.cpu_procs)
+        r = cpu_baseline(w, args.cpu_procs, sample_nt=args.ref_sample_nt)
         if i >= W:
             vals.append(r)
     value = statistics.median(v["value"] for v in vals)
@@ -344,8 +550,7 @@ def run_reference(args):
     out = {"metric": METRIC, "value": value, "unit": "shots/hour", "n_gpus": world,
            "steps": K, "warmup": W, "higher_is_better": True, "impl": "reference",
            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-           "config": {"workload": "751x2301 h=4 m, npml 40, nt 7500 @ 0.4 ms, 576 receivers, "
-                                  "15 Hz, 20 MINRES iterations, datum at 1200 m"},
+           "config": {"workload": workload_text(w, args)},
            "cpu_baseline": {"value": value, "unit": "shots/hour", "cores": r["cores"],
                             "kind": "port", "sample": r["sample"]},
            "e2e": {"value": value, "unit": "shots/hour", "h2d_bytes_per_step": 0,
@@ -360,20 +565,28 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--batch", type=int, default=2)
+    ap.add_argument("--config", type=int, default=4, choices=[2, 4])
+    ap.add_argument("--batch", type=int, default=2, help="--config 2: shots per batch")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-accuracy", action="store_true")
     ap.add_argument("--cpu-procs", type=int, default=None)
-    # profiling variants of the same workload (shorter records / fewer
+    # reference arm: truncated record of each CPU sample (one per step)
+    ap.add_argument("--ref-sample-nt", type=int, default=40)
+    # profiling variants of the uniform workload (shorter records / fewer
     # iterations, same grid and kernels); a line printed with them is marked
     ap.add_argument("--nt", type=int, default=7500)
     ap.add_argument("--maxiter", type=int, default=None)
     ap.add_argument("--no-e2e", action="store_true")
+    # A/B: the one-kernel-per-step path (default) or the split p / v kernels
+    ap.add_argument("--kernel", default="step", choices=["step", "split"])
     # stage-A history in windows of K steps (checkpointed; one shot per launch)
     ap.add_argument("--checkpoint", type=int, default=0)
     args = ap.parse_args()
-    if args.checkpoint > 0 and args.batch != 1:
-        ap.error("--checkpoint runs one shot per launch: give --batch 1")
+    if args.checkpoint > 0 and (args.batch != 1 or args.config != 2):
+        ap.error("--checkpoint runs one shot per launch: give --config 2 --batch 1")
+    if (args.nt != 7500 or args.maxiter is not None) and args.config != 2:
+        ap.error("--nt / --maxiter are profiling variants of --config 2")
     if args.impl == "reference":
         run_reference(args)
     else:

@@ -209,7 +209,9 @@ typedef struct daw_shot_out {   /* every pointer may be NULL */
 int daw_shot(daw_handle* h, const daw_shot_desc* desc, daw_shot_out* out);
 
 /* Batched: n shots (uneven nt, receiver spreads and sources allowed) run in
- * shared launches, batch size admitted by HBM footprint.  outs[i] pairs with
+ * shared launches.  Batches are formed in order: each takes the longest run
+ * of the remaining shots whose device bytes (each shot's own record length
+ * and receiver count) fit ~92 % of the free HBM.  outs[i] pairs with
  * descs[i]. */
 int daw_shots(daw_handle* h, int32_t n, const daw_shot_desc* descs, daw_shot_out* outs);
 
@@ -243,6 +245,10 @@ typedef struct daw_timing {
   double point_updates;       /* extended-grid point updates performed */
   double hist_bytes;          /* history bytes written + read */
   int64_t kernel_launches;    /* kernels launched by the library */
+  double shot_steps_fwd, shot_steps_a, shot_steps_b;  /* shot time steps by kind */
+  /* one-kernel-per-step path: tile columns and CTAs per SM of the last run of
+   * each mode (forward, stage A, stage B, final esource; 0 = not run) */
+  int32_t tile_cols[4], ctas_per_sm[4];
 } daw_timing;
 int daw_get_timing(const daw_handle* h, daw_timing* t);
 void daw_reset_timing(daw_handle* h);

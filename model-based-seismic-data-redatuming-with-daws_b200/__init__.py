@@ -75,7 +75,9 @@ class Timing(C.Structure):
                 ("sim_fwd_ms", C.c_double), ("sim_a_ms", C.c_double), ("sim_b_ms", C.c_double),
                 ("steps_fwd", C.c_double), ("steps_a", C.c_double), ("steps_b", C.c_double),
                 ("shot_steps", C.c_double), ("point_updates", C.c_double), ("hist_bytes", C.c_double),
-                ("kernel_launches", C.c_int64)]
+                ("kernel_launches", C.c_int64), ("shot_steps_fwd", C.c_double),
+                ("shot_steps_a", C.c_double), ("shot_steps_b", C.c_double),
+                ("tile_cols", C.c_int32 * 4), ("ctas_per_sm", C.c_int32 * 4)]
 
 
 _lib = None
@@ -374,7 +376,11 @@ class Handle:
     def timing(self) -> dict:
         t = Timing()
         self._ck(lib().daw_get_timing(self._h, C.byref(t)))
-        return {k: getattr(t, k) for k, _ in Timing._fields_}
+        out = {}
+        for k, _ in Timing._fields_:
+            v = getattr(t, k)
+            out[k] = list(v) if isinstance(v, C.Array) else v
+        return out
 
     def reset_timing(self):
         lib().daw_reset_timing(self._h)

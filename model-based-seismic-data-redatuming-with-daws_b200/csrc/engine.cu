@@ -691,6 +691,8 @@ void stop_clock(daw_handle* h, SimClock& clk, Batch& b, int mode, const Window* 
     if (c->active) shot_steps += w ? w->len : c->nt;
   double* ms = mode == FM_FWD ? &h->tim.sim_fwd_ms : mode == FM_STAGE_A ? &h->tim.sim_a_ms : &h->tim.sim_b_ms;
   double* st = mode == FM_FWD ? &h->tim.steps_fwd : mode == FM_STAGE_A ? &h->tim.steps_a : &h->tim.steps_b;
+  (mode == FM_FWD ? h->tim.shot_steps_fwd : mode == FM_STAGE_A ? h->tim.shot_steps_a
+                                                                : h->tim.shot_steps_b) += shot_steps;
   clk.stop(ms, st, w ? w->len : b.max_nt, shot_steps);
 }
 
@@ -817,6 +819,8 @@ void run_fused(daw_handle* h, Batch& b, int mode, const Window* w = nullptr) {
     L.ngath = mode == FM_STAGE_A ? 0 : (L.max_rec + (b.no_datum ? 0 : L.max_datum) + 7) / 8;
     const daw_handle::Tuned t = tune_step(h, b, mode, L, first);
     h->last_tuned = t;
+    h->tim.tile_cols[mode] = t.tile_cols;
+    h->tim.ctas_per_sm[mode] = t.ctas_per_sm;
     L.tile_cols = t.tile_cols;
     L.smaps = b.d_smaps + (t.tile_cols == 32 ? b.shots.size() : 0);
     grid = t.ctas_per_sm * h->sms;
@@ -1547,27 +1551,39 @@ int history_window(daw_handle* h, int nt, int nr, bool want_wf, size_t avail) {
                                   std::to_string(avail) + " available"};
 }
 
-// Shots per batch, and in *win the stage-A history window (a shot with a
-// window runs alone).
+// Shots of the next batch: the longest prefix of d[0..n) whose shots -- each
+// with its own record length and receiver count -- fit the admission bound
+// together (at most DAW_OPT_MAX_BATCH).  *win is the stage-A history window,
+// set when the first shot alone needs one; a shot with a window runs alone.
 int admit_batch(daw_handle* h, int n, const daw_shot_desc* d, bool want_wf, int* win) {
   *win = 0;
-  if (!h->opt.fused) return 1;
-  int max_nt = 0, max_nr = 0;
-  for (int i = 0; i < n; ++i) {
-    max_nt = std::max(max_nt, d[i].nt);
-    max_nr = std::max(max_nr, d[i].nrec);
-  }
+  if (!h->opt.fused || n <= 0) return std::min(n, 1);
   const size_t avail = admission_bytes(h);
-  *win = history_window(h, max_nt, max_nr, want_wf, avail);
+  *win = history_window(h, d[0].nt, d[0].nrec, want_wf, avail);
   if (*win > 0) return 1;
-  const size_t per = shot_bytes(h, max_nt, max_nr, h->opt.history_fp16, want_wf);
-  int s = (int)(avail / std::max<size_t>(per, 1));
+  const bool fp16 = h->opt.history_fp16 != 0;
+  const int cap = h->opt.max_batch > 0 ? std::min(n, h->opt.max_batch) : n;
+  size_t sum = 0;
+  int s = 0;
+  while (s < cap) {
+    const size_t b = shot_bytes(h, d[s].nt, d[s].nrec, fp16, want_wf);
+    if (sum + b > avail) break;
+    sum += b;
+    ++s;
+  }
   if (s < 1)
-    throw DawError{DAW_ERR_OOM, "HBM admission refused: one shot needs " + std::to_string(per) +
+    throw DawError{DAW_ERR_OOM, "HBM admission refused: one shot needs " +
+                                    std::to_string(shot_bytes(h, d[0].nt, d[0].nrec, fp16, want_wf)) +
                                     " bytes, " + std::to_string(avail) + " available"};
-  s = std::min(s, n);
-  if (h->opt.max_batch > 0) s = std::min(s, h->opt.max_batch);
   return s;
+}
+
+// Frees the per-slot buffers (state, histories, data, MINRES vectors, maps)
+// of the previous batch, so that a batch of differently sized shots
+// allocates exactly what it needs; graphs that point at them go first.
+void release_slots(daw_handle* h) {
+  drop_graphs(h);
+  for (const char* p : {"slot", "shot", "mr", "batch."}) h->pool.release_prefix(p);
 }
 
 void run_shots(daw_handle* h, int n, const daw_shot_desc* descs, daw_shot_out* outs) {
@@ -1575,12 +1591,10 @@ void run_shots(daw_handle* h, int n, const daw_shot_desc* descs, daw_shot_out* o
   if (n <= 0) return;
   bool want_wf = false;
   for (int i = 0; i < n; ++i) want_wf |= (outs && outs[i].wavefield_exd != nullptr);
-  int win = 0;
-  const int S = admit_batch(h, n, descs, want_wf, &win);
-  // Free per-slot buffers beyond the admitted batch size and stale graphs.
-  drop_graphs(h);
-  for (int first = 0; first < n; first += S) {
-    const int cnt = std::min(S, n - first);
+  for (int first = 0; first < n;) {
+    release_slots(h);
+    int win = 0;
+    const int cnt = admit_batch(h, n - first, descs + first, want_wf, &win);
     std::vector<ShotCtx> ctx(cnt);
     Batch b;
     b.slot0 = 0;
@@ -1592,6 +1606,7 @@ void run_shots(daw_handle* h, int n, const daw_shot_desc* descs, daw_shot_out* o
     run_pipeline(h, b);
     for (int i = 0; i < cnt; ++i) fetch_outputs(h, ctx[i], outs ? &outs[first + i] : nullptr);
     drop_graphs(h);
+    first += cnt;
   }
 }
 
@@ -2080,11 +2095,13 @@ int daw_stage_shots(daw_handle* h, int32_t n, const daw_shot_desc* descs) {
     require_model(h);
     if (n <= 0 || !descs) throw DawError{DAW_ERR_ARG, "daw_stage_shots: bad arguments"};
     int win = 0;
+    h->staged_ready = 0;
+    h->staged_ctx.clear();
+    release_slots(h);
     const int S = admit_batch(h, n, descs, false, &win);
     if (S < n)
       throw DawError{DAW_ERR_OOM, "staged shots must fit one batch (" + std::to_string(S) +
                                       " admitted of " + std::to_string(n) + ")"};
-    drop_graphs(h);
     h->staged_ctx.assign(n, ShotCtx());
     for (int i = 0; i < n; ++i)
       prepare_shot(h, h->staged_ctx[i], descs[i], i, false, h->opt.history_fp16 != 0, false, win);
