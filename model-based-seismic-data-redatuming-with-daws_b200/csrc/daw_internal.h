@@ -71,6 +71,10 @@ struct ModelDev {
   float* d2a = nullptr; float* d2b = nullptr;   // damp2a, damp2b (n2e)
   float* d1a1 = nullptr; float* d2a1 = nullptr; // damp1a1, damp2a1
   float* bw1 = nullptr; float* bw2 = nullptr;   // dtdx*1*damp1b1, dtdx*1*damp2b1
+  // The same profiles packed for one load per row / column:
+  // prow[i1] = (d1a, d1a1, d1b, bw1), pcol[i2] = (d2a, d2a1, d2b, bw2).
+  float4* prow = nullptr;
+  float4* pcol = nullptr;
 };
 
 // A set of Hicks stations (sources or receivers) on the device.

@@ -815,6 +815,9 @@ void run_fused(daw_handle* h, Batch& b, int mode, const Window* w = nullptr) {
     L.par0 = std::max(par0, 0);
     L.first = first;
     L.step_last = nt_v;
+    L.active_mask = 0;
+    for (size_t i = 0; i < b.shots.size() && i < 64; ++i)
+      if (b.shots[i]->active) L.active_mask |= 1ull << i;
     L.qctr = h->d_qctr;
     L.ngath = mode == FM_STAGE_A ? 0 : (L.max_rec + (b.no_datum ? 0 : L.max_datum) + 7) / 8;
     const daw_handle::Tuned t = tune_step(h, b, mode, L, first);
@@ -847,10 +850,10 @@ void run_fused(daw_handle* h, Batch& b, int mode, const Window* w = nullptr) {
   if (h->opt.graph && (!w || step)) {
     char key[320];
     std::snprintf(key, sizeof key,
-                  "m%d.n%d.s%zu.p%p.q%p.z%p.c%d.f%d.r%d.d%d.h%llx.w%d.%d.%d.%d.%d.%d.%d",
+                  "m%d.n%d.s%zu.p%p.q%p.z%p.c%d.f%d.r%d.d%d.h%llx.w%d.%d.%d.%d.%d.%d.%d.a%llx",
                   mode, b.max_nt, b.shots.size(), (void*)b.d_shots, (void*)b.d_maps,
                   (void*)b.d_smaps, L.chunk, L.hist_fp16, L.max_rec, L.max_datum, phash, step,
-                  first, last, L.hist_step0, L.par0, L.tile_cols, grid);
+                  first, last, L.hist_step0, L.par0, L.tile_cols, grid, L.active_mask);
     auto it = h->graphs.find(key);
     if (it == h->graphs.end()) {
       cudaGraph_t graph;
@@ -1858,6 +1861,13 @@ int daw_set_model(daw_handle* h, const float* vp, int32_t n1, int32_t n2, int32_
     upload(m.d1a1, d1a1.data(), g.n1e * 4, h->st); upload(m.bw1, bw1.data(), g.n1e * 4, h->st);
     upload(m.d2a, d2a.data(), g.n2e * 4, h->st); upload(m.d2b, d2b.data(), g.n2e * 4, h->st);
     upload(m.d2a1, d2a1.data(), g.n2e * 4, h->st); upload(m.bw2, bw2.data(), g.n2e * 4, h->st);
+    std::vector<float4> prow(g.n1e), pcol(g.n2e);
+    for (int i = 0; i < g.n1e; ++i) prow[i] = make_float4(d1a[i], d1a1[i], d1b[i], bw1[i]);
+    for (int j = 0; j < g.n2e; ++j) pcol[j] = make_float4(d2a[j], d2a1[j], d2b[j], bw2[j]);
+    m.prow = P.get_t<float4>("prow", g.n1e);
+    m.pcol = P.get_t<float4>("pcol", g.n2e);
+    upload(m.prow, prow.data(), g.n1e * sizeof(float4), h->st);
+    upload(m.pcol, pcol.data(), g.n2e * sizeof(float4), h->st);
     sync(h);
     h->g = g;
     h->md = m;

@@ -90,6 +90,7 @@ struct FusedLaunch {
   unsigned* qctr;
   int first, par0, tile_cols, ngath;
   int step_last;  // last stencil step of the run (the extra launch after it does none)
+  unsigned long long active_mask;  // bit i: shot i (< 64) takes part in the run
   static constexpr int kParamShots = 8;
   int nparam;
   const unsigned* shot_amax[kParamShots];

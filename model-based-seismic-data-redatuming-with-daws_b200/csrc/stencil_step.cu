@@ -55,6 +55,7 @@ constexpr int kHPRows = 80;      // rows of the stage-B pressure-history box (st
 constexpr int kAmpMaxS = 2048;   // stations whose amplitudes are staged in shared memory
 constexpr int kBatchS = 6;       // injection entries loaded per point at once
 constexpr int kMaxBandCols = 40; // >= TC + 3
+constexpr int kBandInts = 4 * kMaxBandCols + 8;  // band info of one stage
 constexpr int kGatherStride = 444;
 
 __host__ __device__ constexpr int pad128(int x) { return (x + 127) / 128 * 128; }
@@ -84,7 +85,7 @@ struct SG {
     return (mode == FM_FWD || mode == FM_STAGE_A) ? kAmpMaxS * 4 : 0;
   }
   static constexpr size_t smem(int mode, bool fp16) {
-    return 2 * (size_t)stage(mode, fp16) + amp_bytes(mode) + 5 * kMaxBandCols * 4 + 64;
+    return 2 * (size_t)stage(mode, fp16) + amp_bytes(mode) + 2 * kBandInts * 4 + 64;
   }
   static_assert(2 * kBase >= 8 * kGatherStride * 4, "gather products fit in the stage buffers");
 };
@@ -117,6 +118,9 @@ __device__ __forceinline__ SItem item_of(const Grid& g, int idx, int nshots, int
 
 __device__ __forceinline__ int shot_nt(const FusedLaunch& L, int s) {
   return s < L.nparam ? L.shot_nt[s] : L.shots[s].nt;
+}
+__device__ __forceinline__ bool shot_active(const FusedLaunch& L, int s) {
+  return s < 64 ? ((L.active_mask >> s) & 1ull) != 0 : L.shots[s].active != 0;
 }
 
 // What launch `it` does for a shot of record length nt (all threads agree).
@@ -218,7 +222,7 @@ __device__ __forceinline__ float warp_gather_pxpz(float* prod, const int* ix1p, 
 }
 
 template <int MODE, bool FP16, int TC>
-__global__ void __launch_bounds__(kT, 2)
+__global__ void __launch_bounds__(kT, TC == 16 ? 3 : 2)
     k_step(const Grid g, const ModelDev m, const FusedLaunch L, const int it) {
   using G = SG<TC>;
   using H = Hist<FP16>;
@@ -228,12 +232,11 @@ __global__ void __launch_bounds__(kT, 2)
   constexpr bool kInj = (MODE == FM_FWD || MODE == FM_STAGE_A);
   extern __shared__ __align__(128) unsigned char smem[];
   float* amp_s = reinterpret_cast<float*>(smem + 2 * kStage);
-  int* binfo = reinterpret_cast<int*>(smem + 2 * kStage + G::amp_bytes(MODE));  // 5 x kMaxBandCols
-  int* b_lo = binfo;                                        // first band row (clipped)
-  int* b_olo = binfo + kMaxBandCols;                        // col_lo of the map
-  int* b_base = binfo + 2 * kMaxBandCols;                   // col_base of the map
-  int* b_pre = binfo + 3 * kMaxBandCols;                    // prefix of band points
-  uint64_t* bar = reinterpret_cast<uint64_t*>(binfo + 5 * kMaxBandCols);
+  // injection band of the tile in each stage (written one item ahead):
+  // per box column the first band row (clipped), the map's col_lo and
+  // col_base, the prefix of band points, then the count of band points
+  int* binfo0 = reinterpret_cast<int*>(smem + 2 * kStage + G::amp_bytes(MODE));
+  uint64_t* bar = reinterpret_cast<uint64_t*>(binfo0 + 2 * kBandInts);
   int* item_s = reinterpret_cast<int*>(bar + 2);            // item of each stage
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   if (tid == 0) {
@@ -280,17 +283,80 @@ __global__ void __launch_bounds__(kT, 2)
              pol);
     }
   };
-  // Thread 0 takes the next item and, for a tile that needs it, issues its copies.
-  auto grab = [&](int s) {
-    const int idx = (int)(atomicAdd(L.qctr, 1u) - qbase);
-    item_s[s] = idx;
+  // Thread 0 takes items from the queue two ahead of the one the CTA works
+  // on, so the atomic's latency hides behind a tile; it stops after the first
+  // index past the end (one such index per CTA and launch).
+  auto take = [&]() { return (int)(atomicAdd(L.qctr, 1u) - qbase); };
+  auto issue_if_tile = [&](int idx, int s) {
     const SItem id = item_of<TC>(g, idx, L.nshots, ntile, ngath);
-    if (id.kind == 0) {
-      const ShotStep ss = shot_step<MODE>(L, shot_nt(L, id.shot), true, it);
-      if (needs_tile<MODE>(ss) && L.shots[id.shot].active) issue(id, s);
-    }
+    if (id.kind != 0 || !shot_active(L, id.shot)) return;
+    const ShotStep ss = shot_step<MODE>(L, shot_nt(L, id.shot), true, it);
+    if (needs_tile<MODE>(ss)) issue(id, s);
   };
-  if (tid == 0) grab(0);
+  // Band of the injection map at the tile's pressure points (warp 0): the
+  // loads are issued when the tile is next in line, the counts and prefix
+  // are stored into its stage's band info at the end of the current item.
+  struct BandLoads {
+    int olo[2], ohi[2], base[2];
+  };
+  auto band_load = [&](const SItem& id, const InjMapDev& mp) {
+    BandLoads r;
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int cc = lane + 32 * h;  // box column: global column c0 - 1 + cc
+      const int c = id.c0 - 1 + cc;
+      const bool ok = cc < NP && c >= 0 && c < n2e;
+      r.olo[h] = ok ? __ldg(mp.col_lo + c) : 0x7fffffff;
+      r.ohi[h] = ok ? __ldg(mp.col_hi + c) : -1;
+      r.base[h] = ok ? __ldg(mp.col_base + c) : 0;
+    }
+    return r;
+  };
+  auto band_store = [&](const SItem& id, const BandLoads& r, int slot) {
+    int* bi = binfo0 + slot * kBandInts;
+    int cnt[2];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int cc = lane + 32 * h;
+      const bool tcol = cc >= 1 && cc <= TC;
+      const int dlo = tcol ? id.r0 - 1 : id.r0;
+      const int dhi = min(tcol ? id.r0 + SR + 1 : id.r0 + SR - 1, n1e - 1);
+      const int lo = max(r.olo[h], max(dlo, 0));
+      const int hi = min(r.ohi[h], dhi);
+      cnt[h] = hi >= lo ? hi - lo + 1 : 0;
+      if (cc < kMaxBandCols) {
+        bi[cc] = lo;
+        bi[kMaxBandCols + cc] = r.olo[h];
+        bi[2 * kMaxBandCols + cc] = r.base[h];
+      }
+    }
+    int incl0 = cnt[0], incl1 = cnt[1];
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y0 = __shfl_up_sync(kAll, incl0, o);
+      const int y1 = __shfl_up_sync(kAll, incl1, o);
+      if (lane >= o) {
+        incl0 += y0;
+        incl1 += y1;
+      }
+    }
+    const int tot0 = __shfl_sync(kAll, incl0, 31);
+    const int tot1 = __shfl_sync(kAll, incl1, 31);
+    bi[3 * kMaxBandCols + lane] = incl0 - cnt[0];
+    if (lane + 32 < kMaxBandCols) bi[3 * kMaxBandCols + lane + 32] = tot0 + incl1 - cnt[1];
+    if (lane == 0) bi[4 * kMaxBandCols] = tot0 + tot1;
+  };
+  if (tid == 0) {
+    const int i0 = take();
+    item_s[0] = i0;
+    item_s[1] = i0 < nitems ? take() : nitems;
+    issue_if_tile(i0, 0);
+  }
+  __syncthreads();
+  if (kInj && warp == 0) {
+    const SItem i0 = item_of<TC>(g, item_s[0], L.nshots, ntile, ngath);
+    if (i0.kind == 0) band_store(i0, band_load(i0, L.shots[i0.shot].inj), 0);
+  }
   __syncthreads();
 
   uint32_t phase[2] = {0, 0};
@@ -317,10 +383,15 @@ __global__ void __launch_bounds__(kT, 2)
 
   for (int k = 0;; ++k) {
     const int s = k & 1;
-    const int idx = item_s[s];
-    const SItem id = item_of<TC>(g, idx, L.nshots, ntile, ngath);
+    const SItem id = item_of<TC>(g, item_s[s], L.nshots, ntile, ngath);
     if (id.kind == 2) break;
-    if (tid == 0) grab(s ^ 1);
+    const int nidx = item_s[s ^ 1];
+    const SItem nxt = item_of<TC>(g, nidx, L.nshots, ntile, ngath);
+    int pend = nitems;  // item k + 2 (thread 0)
+    if (tid == 0) {
+      issue_if_tile(nidx, s ^ 1);
+      if (nidx < nitems) pend = take();
+    }
     if (id.shot != cur) {  // CTA-uniform: shot set-up
       flush_amax();
       __syncthreads();  // every thread is done with the previous descriptor
@@ -358,6 +429,11 @@ __global__ void __launch_bounds__(kT, 2)
       }
       __syncthreads();
     }
+    // band loads of the next tile, stored at the end of this item
+    const bool nb_on = kInj && warp == 0 && nxt.kind == 0;
+    BandLoads nb;
+    if (nb_on) nb = band_load(nxt, nxt.shot == cur ? sd.inj : L.shots[nxt.shot].inj);
+    do {  // the item; `break` ends it
     if (id.kind == 1) {
       // ---- gather unit: receivers / datum of step it - 1 from the input set
       if (ss.defer && MODE != FM_STAGE_A) {
@@ -383,68 +459,22 @@ __global__ void __launch_bounds__(kT, 2)
           if (lane == 0) sd.red[(step - 1) + (size_t)sd.nt * d] = v;
         }
       }
-      __syncthreads();
-      continue;
+      break;
     }
     // ---- tile
-    if (!(needs_tile<MODE>(ss) && active)) {
-      __syncthreads();
-      continue;
-    }
+    if (!(needs_tile<MODE>(ss) && active)) break;
     const int r0 = id.r0, c0 = id.c0;
     const bool interior = step_interior<TC>(g, r0, c0, MODE, slo, shi1, shi2);
     // Injection band of the tile's pressure points (forward source / stage-A
-    // receivers): per box column, the clipped band rows and their count.
+    // receivers), stored with the previous item: per box column, the clipped
+    // band rows; their total count.
     const bool inj = kInj && ss.step && (MODE == FM_STAGE_A || sd.type_src == 0);
-    int nband = 0;
-    if (inj) {
-      if (warp == 0) {
-        int cnt[2] = {0, 0};
-#pragma unroll
-        for (int h = 0; h < 2; ++h) {
-          const int cc = lane + 32 * h;  // box column: global column c0 - 1 + cc
-          const int c = c0 - 1 + cc;
-          int lo = 0, olo = 0, base = 0;
-          if (cc < NP && c >= 0 && c < n2e) {
-            olo = __ldg(sd.inj.col_lo + c);
-            const int ohi = __ldg(sd.inj.col_hi + c);
-            base = __ldg(sd.inj.col_base + c);
-            const bool tcol = cc >= 1 && cc <= TC;
-            const int dlo = tcol ? r0 - 1 : r0, dhi = min(tcol ? r0 + SR + 1 : r0 + SR - 1, n1e - 1);
-            lo = max(olo, max(dlo, 0));
-            const int hi = min(ohi, dhi);
-            cnt[h] = hi >= lo ? hi - lo + 1 : 0;
-          }
-          if (cc < kMaxBandCols) {
-            b_lo[cc] = lo;
-            b_olo[cc] = olo;
-            b_base[cc] = base;
-          }
-        }
-        // exclusive prefix over the box columns (lane handles cc and cc + 32)
-        int v0 = cnt[0];
-        int incl = v0;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-          const int y = __shfl_up_sync(kAll, incl, o);
-          if (lane >= o) incl += y;
-        }
-        const int tot0 = __shfl_sync(kAll, incl, 31);
-        int v1 = cnt[1];
-        int incl1 = v1;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-          const int y = __shfl_up_sync(kAll, incl1, o);
-          if (lane >= o) incl1 += y;
-        }
-        b_pre[lane] = incl - v0;
-        if (lane + 32 < kMaxBandCols) b_pre[lane + 32] = tot0 + incl1 - v1;
-        const int tot1 = __shfl_sync(kAll, incl1, 31);
-        if (lane == 0) binfo[4 * kMaxBandCols] = tot0 + tot1;
-      }
-      __syncthreads();
-      nband = binfo[4 * kMaxBandCols];
-    }
+    const int* bi = binfo0 + s * kBandInts;
+    const int* b_lo = bi;
+    const int* b_olo = bi + kMaxBandCols;
+    const int* b_base = bi + 2 * kMaxBandCols;
+    const int* b_pre = bi + 3 * kMaxBandCols;
+    const int nband = inj ? bi[4 * kMaxBandCols] : 0;
     const int i1 = r0 + 2 * lane;
     const int cb = c0 + CPT * warp;
     bar_wait(&bar[s], phase[s], L.err);
@@ -513,14 +543,13 @@ __global__ void __launch_bounds__(kT, 2)
           float d2a = 1.f, d2a1 = 1.f;
           float2 d1a = make_float2(1.f, 1.f), d1a1 = make_float2(1.f, 1.f);
           if (!IN) {
-            d2a = __ldg(m.d2a + c);
-            d2a1 = __ldg(m.d2a1 + c);
-            d1a.x = __ldg(m.d1a + i1);
-            d1a1.x = __ldg(m.d1a1 + i1);
-            if (ok1_) {
-              d1a.y = __ldg(m.d1a + i1 + 1);
-              d1a1.y = __ldg(m.d1a1 + i1 + 1);
-            }
+            const float4 pc4 = __ldg(m.pcol + c);
+            const float4 r04 = __ldg(m.prow + i1);
+            const float4 r14 = ok1_ ? __ldg(m.prow + i1 + 1) : r04;
+            d2a = pc4.x;
+            d2a1 = pc4.y;
+            d1a = make_float2(r04.x, r14.x);
+            d1a1 = make_float2(r04.y, r14.y);
           }
           if (u0_) {
             const float der2 = dminus(q[j].x, q[j + 1].x, q[j + 2].x, q[j + 3].x);
@@ -625,10 +654,11 @@ __global__ void __launch_bounds__(kT, 2)
           if (IN) {
             ax = px_; bx = fmul(kd, der2); az = pz_; bz = fmul(kd, der1);
           } else {
-            ax = fmul(__ldg(m.d2a + c), px_);
-            bx = fmul(fmul(kd, __ldg(m.d2a1 + c)), der2);
-            az = fmul(__ldg(m.d1a + i), pz_);
-            bz = fmul(fmul(kd, __ldg(m.d1a1 + i)), der1);
+            const float4 pc4 = __ldg(m.pcol + c), pr4 = __ldg(m.prow + i);
+            ax = fmul(pc4.x, px_);
+            bx = fmul(fmul(kd, pc4.y), der2);
+            az = fmul(pr4.x, pz_);
+            bz = fmul(fmul(kd, pr4.y), der1);
           }
           px_ = fwd ? fadd(ax, bx) : fsub(ax, bx);
           pz_ = fwd ? fadd(az, bz) : fsub(az, bz);
@@ -811,14 +841,13 @@ __global__ void __launch_bounds__(kT, 2)
             float d2b = 1.f, bw2 = dtdx_v;
             float2 d1b = make_float2(1.f, 1.f), bw1 = make_float2(dtdx_v, dtdx_v);
             if (!IN) {
-              d2b = __ldg(m.d2b + c);
-              bw2 = __ldg(m.bw2 + c);
-              d1b.x = __ldg(m.d1b + i1);
-              bw1.x = __ldg(m.bw1 + i1);
-              if (ok1_) {
-                d1b.y = __ldg(m.d1b + i1 + 1);
-                bw1.y = __ldg(m.bw1 + i1 + 1);
-              }
+              const float4 pc4 = __ldg(m.pcol + c);
+              const float4 r04 = __ldg(m.prow + i1);
+              const float4 r14 = ok1_ ? __ldg(m.prow + i1 + 1) : r04;
+              d2b = pc4.z;
+              bw2 = pc4.w;
+              d1b = make_float2(r04.z, r14.z);
+              bw1 = make_float2(r04.w, r14.w);
             }
             if (u0_) {
               const float der2 = dplus(a[j].x, pcv.x, a[j + 2].x, a[j + 3].x);
@@ -900,7 +929,10 @@ __global__ void __launch_bounds__(kT, 2)
       else
         v_pass(std::false_type{});
     }
-    __syncthreads();  // stage free for the copies of item k + 2
+    } while (false);
+    if (nb_on) band_store(nxt, nb, s ^ 1);
+    if (tid == 0) item_s[s] = pend;
+    __syncthreads();  // stage s free for the copies of item k + 2
   }
   flush_amax();
 }
