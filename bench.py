@@ -371,7 +371,8 @@ def run_ours(args):
     mine = list(range(ista - 1, iend))
     cap = args.batch if args.config == 2 else 8
     h = pkg.Handle(local, preset="mixed", checkpoint=args.checkpoint,
-                   step=1 if args.kernel == "step" else 0)
+                   step=1 if args.kernel == "step" else 0, tile_cols=args.tile_cols,
+                   ctas_per_sm=args.ctas_per_sm)
     if args.config == 2:
         per_step = args.batch
         need = per_step
@@ -580,6 +581,9 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     # A/B: the one-kernel-per-step path (default) or the split p / v kernels
     ap.add_argument("--kernel", default="step", choices=["step", "split"])
+    # pin the step kernel's tile width / CTAs per SM (0 = autotuned)
+    ap.add_argument("--tile-cols", type=int, default=0, choices=[0, 16, 32])
+    ap.add_argument("--ctas-per-sm", type=int, default=0)
     # stage-A history in windows of K steps (checkpointed; one shot per launch)
     ap.add_argument("--checkpoint", type=int, default=0)
     args = ap.parse_args()
