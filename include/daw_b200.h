@@ -74,15 +74,18 @@ enum daw_option {
                                 from that state while stage B consumes the windows in
                                 reverse order.  No counterpart in the reference, which
                                 keeps whole histories. */,
-  DAW_OPT_STEP_KERNEL = 9,   /* TMA kernels (DAW_OPT_CHUNK = 0): 1 (default) = one
-                                kernel per time step (pressure recomputed on the
-                                velocity stencil's halo, two alternating state sets);
-                                0 = separate pressure and velocity kernels */
+  DAW_OPT_STEP_KERNEL = 9,   /* TMA kernels (DAW_OPT_CHUNK = 0): 0 (default) = separate
+                                pressure and velocity kernels; 1 = one kernel per time
+                                step (pressure recomputed on the velocity stencil's
+                                halo, two alternating state sets) */
   DAW_OPT_TILE_COLS = 10,    /* one-kernel-per-step tiles: 16 or 32 columns of 64
                                 rows; 0 (default) = chosen by the autotuner */
-  DAW_OPT_CTAS_PER_SM = 11   /* one-kernel-per-step CTAs per SM (1..3; a value above
+  DAW_OPT_CTAS_PER_SM = 11,  /* one-kernel-per-step CTAs per SM (1..3; a value above
                                 what fits is lowered to the occupancy); 0 (default) =
                                 chosen by the autotuner */
+  DAW_OPT_PDL = 12           /* TMA kernels: 1 (default) = programmatic dependent launch
+                                (a time step's kernel starts launching while the
+                                previous one drains); 0 = plain stream order */
 };
 
 /* Handle lifetime ------------------------------------------------------- */

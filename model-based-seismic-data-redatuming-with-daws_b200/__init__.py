@@ -36,7 +36,7 @@ STATUS = {0: "OK", -1: "ERR_ARG", -2: "ERR_OOM", -3: "ERR_CUDA", -4: "ERR_TIMEOU
           -5: "ERR_NAN", -6: "ERR_IO", -7: "ERR_STATE", -8: "ERR_NODEV"}
 OPT = {"preset": 0, "history": 1, "scalars": 2, "fused": 3, "graph": 4, "skip_dead_op": 5,
        "max_batch": 6, "chunk": 7, "checkpoint": 8, "step": 9, "tile_cols": 10,
-       "ctas_per_sm": 11}
+       "ctas_per_sm": 11, "pdl": 12}
 
 
 class DawError(RuntimeError):

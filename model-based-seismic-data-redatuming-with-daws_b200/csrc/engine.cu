@@ -650,8 +650,12 @@ void fill_shot_devices(daw_handle* h, Batch& b, int mode, const Window* w = null
                            h->opt.history_fp16, hist_ld(h), c.hist_steps, &maps[i]))
         throw DawError{DAW_ERR_CUDA, "cuTensorMapEncodeTiled failed"};
     }
+    // one buffer per mode: a buffer's contents then never change between the
+    // launches of a run or a cached graph (windowed runs switch the state
+    // pointers between stage A and stage B)
     b.d_maps = static_cast<TmaMaps*>(
-        h->pool.get("batch.maps" + std::to_string(b.slot0), maps.size() * sizeof(TmaMaps)));
+        h->pool.get("batch.maps" + std::to_string(b.slot0) + "." + std::to_string(mode),
+                    maps.size() * sizeof(TmaMaps)));
     upload(b.d_maps, maps.data(), maps.size() * sizeof(TmaMaps), h->st);
     sync(h);  // `maps` goes out of scope
   }
@@ -670,6 +674,7 @@ FusedLaunch launch_of(daw_handle* h, Batch& b) {
   L.err = h->d_err;
   L.persist_p = h->persist_p;
   L.persist_v = h->persist_v;
+  L.pdl = h->opt.pdl;
   return L;
 }
 
@@ -765,9 +770,9 @@ daw_handle::Tuned tune_step(daw_handle* h, Batch& b, int mode, FusedLaunch L, in
 // With a window (one shot, checkpointed stage A): stage A runs the window as a
 // record of w->len steps; stage B runs the record steps that read the
 // window's history, nt-s0-len+1 .. nt-s0, with history slot 0 = step s0+1.
-// The split kernels launch windowed runs directly; the one-kernel-per-step
-// path captures them in graphs too, keyed by the window's first step, length
-// and history offset and by the state set the run starts from.
+// Windowed runs are captured in graphs too, keyed by the window's first and
+// last step, its history offset and the state set the run starts from; each
+// mode has its own tensor-map buffer, whose contents stay fixed for a stage.
 void run_fused(daw_handle* h, Batch& b, int mode, const Window* w = nullptr) {
   const Grid& g = h->g;
   if (w && b.shots.size() != 1) throw DawError{DAW_ERR_STATE, "a windowed run holds one shot"};
@@ -847,13 +852,13 @@ void run_fused(daw_handle* h, Batch& b, int mode, const Window* w = nullptr) {
   const int nsteps = nt_v - first + 1;
   const long long launches = step ? (long long)nsteps + 1
                                   : 2LL * nsteps + (mode == FM_STAGE_A ? 1 : 0);
-  if (h->opt.graph && (!w || step)) {
+  if (h->opt.graph) {
     char key[320];
     std::snprintf(key, sizeof key,
-                  "m%d.n%d.s%zu.p%p.q%p.z%p.c%d.f%d.r%d.d%d.h%llx.w%d.%d.%d.%d.%d.%d.%d.a%llx",
+                  "m%d.n%d.s%zu.p%p.q%p.z%p.c%d.f%d.r%d.d%d.h%llx.w%d.%d.%d.%d.%d.%d.%d.a%llx.l%d",
                   mode, b.max_nt, b.shots.size(), (void*)b.d_shots, (void*)b.d_maps,
                   (void*)b.d_smaps, L.chunk, L.hist_fp16, L.max_rec, L.max_datum, phash, step,
-                  first, last, L.hist_step0, L.par0, L.tile_cols, grid, L.active_mask);
+                  first, last, L.hist_step0, L.par0, L.tile_cols, grid, L.active_mask, L.pdl);
     auto it = h->graphs.find(key);
     if (it == h->graphs.end()) {
       cudaGraph_t graph;
@@ -1776,6 +1781,7 @@ int daw_set_option(daw_handle* h, int32_t key, double value) {
         h->opt.checkpoint = v;
         break;
       case DAW_OPT_STEP_KERNEL: h->opt.step = v ? 1 : 0; break;
+      case DAW_OPT_PDL: h->opt.pdl = v ? 1 : 0; break;
       case DAW_OPT_TILE_COLS:
         if (v != 0 && v != 16 && v != 32)
           throw DawError{DAW_ERR_ARG, "tile columns must be 16 or 32 (0 = autotuned)"};
@@ -1807,6 +1813,7 @@ int daw_get_option(const daw_handle* h, int32_t key, double* value) {
     case DAW_OPT_CHUNK: *value = o.chunk; break;
     case DAW_OPT_CHECKPOINT: *value = o.checkpoint; break;
     case DAW_OPT_STEP_KERNEL: *value = o.step; break;
+    case DAW_OPT_PDL: *value = o.pdl; break;
     case DAW_OPT_TILE_COLS: *value = o.tile_cols; break;
     case DAW_OPT_CTAS_PER_SM: *value = o.ctas_per_sm; break;
     default: return DAW_ERR_ARG;

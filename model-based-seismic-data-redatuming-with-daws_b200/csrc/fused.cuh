@@ -91,6 +91,7 @@ struct FusedLaunch {
   int first, par0, tile_cols, ngath;
   int step_last;  // last stencil step of the run (the extra launch after it does none)
   unsigned long long active_mask;  // bit i: shot i (< 64) takes part in the run
+  int pdl;  // TMA kernels launched with programmatic dependent launch
   static constexpr int kParamShots = 8;
   int nparam;
   const unsigned* shot_amax[kParamShots];

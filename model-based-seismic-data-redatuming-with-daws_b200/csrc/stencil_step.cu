@@ -244,6 +244,9 @@ __global__ void __launch_bounds__(kT, TC == 16 ? 3 : 2)
     bar_init(&bar[1]);
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   }
+  pdl_trigger();
+  // the previous launch's fields, scales, outputs and queue counts are complete
+  pdl_wait();
   const int hbase = g.hist_base();
   const int ld = g.ld, n1e = g.n1e, n2e = g.n2e, npml = g.npml;
   const int off = (MODE == FM_FWD) ? 2 : 3;
@@ -940,7 +943,8 @@ __global__ void __launch_bounds__(kT, TC == 16 ? 3 : 2)
 template <int MODE, bool FP16, int TC>
 void launch_t(const Grid& g, const ModelDev& m, const FusedLaunch& L, int it, int grid,
               cudaStream_t st) {
-  k_step<MODE, FP16, TC><<<grid, kT, SG<TC>::smem(MODE, FP16), st>>>(g, m, L, it);
+  launch_pdl(k_step<MODE, FP16, TC>, grid, kT, SG<TC>::smem(MODE, FP16), st, L.pdl != 0, g, m, L,
+             it);
 }
 
 template <int MODE, bool FP16>

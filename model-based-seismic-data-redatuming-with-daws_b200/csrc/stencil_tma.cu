@@ -166,7 +166,9 @@ __global__ void __launch_bounds__(kThreadsT, 2)
     bar_init(&bar[1]);
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   }
+  pdl_trigger();
   __syncthreads();
+  pdl_wait();  // the previous step's fields, scales and outputs are complete
   const int hbase = g.hist_base();
   auto issue = [&](int t, int s) {
     const TileId id = tile_id(g, t);
@@ -586,7 +588,9 @@ __global__ void __launch_bounds__(kThreadsT,
     bar_init(&bar[1]);
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   }
+  pdl_trigger();
   __syncthreads();
+  pdl_wait();  // the previous step's fields, scales and outputs are complete
   const int hbase = g.hist_base();
   auto issue = [&](int t, int s) {
     const TileId id = tile_id(g, t);
@@ -841,9 +845,11 @@ void launch_p(const Grid& g, const ModelDev& m, const FusedLaunch& L, int it, cu
   const int ntiles = tma_tiles(g) * L.nshots;
   const int grid = std::min(ntiles, L.persist_p);
   if (L.hist_fp16)
-    k_tma_p<MODE, true><<<grid, kThreadsT, p_smem(MODE, true), st>>>(g, m, L, it, ntiles);
+    launch_pdl(k_tma_p<MODE, true>, grid, kThreadsT, p_smem(MODE, true), st, L.pdl != 0, g, m, L,
+               it, ntiles);
   else
-    k_tma_p<MODE, false><<<grid, kThreadsT, p_smem(MODE, false), st>>>(g, m, L, it, ntiles);
+    launch_pdl(k_tma_p<MODE, false>, grid, kThreadsT, p_smem(MODE, false), st, L.pdl != 0, g, m,
+               L, it, ntiles);
 }
 
 template <int MODE>
@@ -853,9 +859,11 @@ void launch_v(const Grid& g, const ModelDev& m, const FusedLaunch& L, int it, cu
   const int ngbps = (stations + 7) / 8;
   const int grid = std::max(1, std::min(std::max(ntiles, ngbps * L.nshots), L.persist_v));
   if (L.hist_fp16)
-    k_tma_v<MODE, true><<<grid, kThreadsT, v_smem(MODE, true), st>>>(g, m, L, it, ntiles, ngbps);
+    launch_pdl(k_tma_v<MODE, true>, grid, kThreadsT, v_smem(MODE, true), st, L.pdl != 0, g, m, L,
+               it, ntiles, ngbps);
   else
-    k_tma_v<MODE, false><<<grid, kThreadsT, v_smem(MODE, false), st>>>(g, m, L, it, ntiles, ngbps);
+    launch_pdl(k_tma_v<MODE, false>, grid, kThreadsT, v_smem(MODE, false), st, L.pdl != 0, g, m,
+               L, it, ntiles, ngbps);
 }
 
 template <typename K>

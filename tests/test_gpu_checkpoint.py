@@ -49,6 +49,7 @@ def test_option_roundtrip(pkg, case):
 # (options, window lengths): nt = 400, so 1 and 399 are the extremes, 7 leaves
 # a last window of 1 step and 100 divides the record.
 GGT_CASES = [({}, (1, 7, 100, 399)), ({"history": 0}, (7, 64)), ({"graph": 0}, (50,)),
+             ({"step": 1}, (7, 100)), ({"step": 1, "history": 0}, (33,)),
              ({"chunk": 2}, (7,)), ({"chunk": 1, "history": 0}, (33,))]
 
 
@@ -74,7 +75,7 @@ def test_windowed_ggt_matches_oracle(pkg, O, case):
     assert np.array_equal(got, ref)
 
 
-@pytest.mark.parametrize("opt", [{}, {"history": 0}])
+@pytest.mark.parametrize("opt", [{}, {"history": 0}, {"step": 1}])
 def test_windowed_esource_bitexact(pkg, case, opt):
     with handle(pkg, case, **opt) as h:
         sis0, wf0, cost0 = h.submodeling_adjoint_esource(case["res"], case["rec"])

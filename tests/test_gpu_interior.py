@@ -93,8 +93,9 @@ def _handle(pkg, w, preset, **opt):
 
 
 PATHS = [("plain", {}), ("mixed", {"history": 0}), ("mixed", {"history": 0, "graph": 0}),
-         ("mixed", {"history": 0, "tile_cols": 16}), ("mixed", {"history": 0, "tile_cols": 32}),
-         ("mixed", {"history": 0, "step": 0}),
+         ("mixed", {"history": 0, "step": 1, "tile_cols": 16}),
+         ("mixed", {"history": 0, "step": 1, "tile_cols": 32}),
+         ("mixed", {"history": 0, "pdl": 0}),
          ("mixed", {"history": 0, "chunk": 1}), ("mixed", {"history": 0, "chunk": 2}),
          ("mixed", {"history": 0, "chunk": 4})]
 
@@ -203,8 +204,8 @@ def test_config2_grid_is_mostly_interior():
 
 @pytest.mark.parametrize("preset,opt", [("plain", {}), ("mixed", {"history": 0}),
                                         ("mixed", {"history": 0, "graph": 0}),
-                                        ("mixed", {"history": 0, "tile_cols": 16}),
-                                        ("mixed", {"history": 0, "step": 0})])
+                                        ("mixed", {"history": 0, "step": 1, "tile_cols": 16}),
+                                        ("mixed", {"history": 0, "pdl": 0})])
 def test_config2_grid_forward_and_ggt_bitexact(pkg, c2, preset, opt):
     w = c2["w"]
     with _handle(pkg, w, preset, **opt) as h:
