@@ -372,7 +372,7 @@ def run_ours(args):
     cap = args.batch if args.config == 2 else 8
     h = pkg.Handle(local, preset="mixed", checkpoint=args.checkpoint,
                    step=1 if args.kernel == "step" else 0, tile_cols=args.tile_cols,
-                   ctas_per_sm=args.ctas_per_sm)
+                   ctas_per_sm=args.ctas_per_sm, pdl=0 if args.no_pdl else 1)
     if args.config == 2:
         per_step = args.batch
         need = per_step
@@ -511,7 +511,8 @@ def run_ours(args):
                        "density": "1 (the reference's rho = 1, src/submodeling2.f90:93)",
                        "kernel": ("one TMA kernel per time step (p recomputed on the v halo)"
                                   if args.kernel == "step" else
-                                  "split TMA pressure and velocity kernels"),
+                                  "TMA pressure and velocity kernels")
+                                 + ("" if args.no_pdl else ", programmatic dependent launch"),
                        "autotuned_tile_cols_ctas_per_sm": tc,
                        "parallelism": f"shots x{world} (para_range, no collective)",
                        "stage_a_history": (f"windows of {args.checkpoint} steps (checkpointed)"
@@ -580,7 +581,8 @@ def main():
     ap.add_argument("--maxiter", type=int, default=None)
     ap.add_argument("--no-e2e", action="store_true")
     # A/B: the one-kernel-per-step path (default) or the split p / v kernels
-    ap.add_argument("--kernel", default="step", choices=["step", "split"])
+    ap.add_argument("--kernel", default="split", choices=["step", "split"])
+    ap.add_argument("--no-pdl", action="store_true", help="plain stream order between steps")
     # pin the step kernel's tile width / CTAs per SM (0 = autotuned)
     ap.add_argument("--tile-cols", type=int, default=0, choices=[0, 16, 32])
     ap.add_argument("--ctas-per-sm", type=int, default=0)
