@@ -83,9 +83,9 @@ enum daw_option {
   DAW_OPT_CTAS_PER_SM = 11,  /* one-kernel-per-step CTAs per SM (1..3; a value above
                                 what fits is lowered to the occupancy); 0 (default) =
                                 chosen by the autotuner */
-  DAW_OPT_PDL = 12           /* TMA kernels: 1 (default) = programmatic dependent launch
-                                (a time step's kernel starts launching while the
-                                previous one drains); 0 = plain stream order */
+  DAW_OPT_PDL = 12           /* TMA kernels: 1 = programmatic dependent launch (a time
+                                step's kernel starts launching while the previous one
+                                drains); 0 (default) = plain stream order */
 };
 
 /* Handle lifetime ------------------------------------------------------- */

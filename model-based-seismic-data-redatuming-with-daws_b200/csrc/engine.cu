@@ -808,6 +808,8 @@ void run_fused(daw_handle* h, Batch& b, int mode, const Window* w = nullptr) {
   // split kernels' extra stage-A launch flushes its history
   const int last = step ? nt_v + 1 : (mode == FM_STAGE_A) ? nt_v + 1 : nt_v;
   const bool tma = L.chunk == 0;
+  L.first = first;
+  L.qctr = h->d_qctr;  // tile queues: [0] pressure / step kernel, [1] velocity kernel
   int grid = 0;
   if (step) {
     int par0 = -1;
@@ -839,6 +841,7 @@ void run_fused(daw_handle* h, Batch& b, int mode, const Window* w = nullptr) {
       for (int it = first; it <= last; ++it) step_launch(g, h->md, L, mode, it, grid, h->st);
       return;
     }
+    if (tma) CK(cudaMemsetAsync(h->d_qctr, 0, 2 * sizeof(unsigned), h->st));
     for (int it = first; it <= last; ++it) {
       if (tma) {
         tma_p_step(g, h->md, L, mode, it, h->st);
@@ -1726,7 +1729,7 @@ int daw_create(daw_handle** out, int32_t device) {
   if (filter_noalloc_prepare(nullptr, 0) != DAW_OK) cudaGetLastError();
   if (cudaMalloc(&h->d_err, sizeof(unsigned)) != cudaSuccess ||
       cudaMemset(h->d_err, 0, sizeof(unsigned)) != cudaSuccess ||
-      cudaMalloc(&h->d_qctr, sizeof(unsigned)) != cudaSuccess || cudaGetLastError() != cudaSuccess) {
+      cudaMalloc(&h->d_qctr, 2 * sizeof(unsigned)) != cudaSuccess || cudaGetLastError() != cudaSuccess) {
     cudaGetLastError();
     cudaStreamDestroy(h->st);
     delete h;
