@@ -809,7 +809,7 @@ void run_fused(daw_handle* h, Batch& b, int mode, const Window* w = nullptr) {
   const int last = step ? nt_v + 1 : (mode == FM_STAGE_A) ? nt_v + 1 : nt_v;
   const bool tma = L.chunk == 0;
   L.first = first;
-  L.qctr = h->d_qctr;  // tile queues: [0] pressure / step kernel, [1] velocity kernel
+  L.qctr = h->d_qctr;  // tile queue of the one-kernel-per-step path
   int grid = 0;
   if (step) {
     int par0 = -1;
@@ -841,7 +841,6 @@ void run_fused(daw_handle* h, Batch& b, int mode, const Window* w = nullptr) {
       for (int it = first; it <= last; ++it) step_launch(g, h->md, L, mode, it, grid, h->st);
       return;
     }
-    if (tma) CK(cudaMemsetAsync(h->d_qctr, 0, 2 * sizeof(unsigned), h->st));
     for (int it = first; it <= last; ++it) {
       if (tma) {
         tma_p_step(g, h->md, L, mode, it, h->st);

@@ -67,12 +67,10 @@ __host__ __device__ constexpr int p_stage(int mode, bool fp16) {
 __host__ __device__ constexpr int v_stage(int mode, bool fp16) {
   return kVStage + ((mode == FM_STAGE_B || mode == FM_STAGE_B_ES) ? 2 * hist_box(fp16) : 0);
 }
-// [stage 0][stage 1][2 mbarriers][amplitudes][queue items]
-constexpr size_t p_smem(int mode, bool fp16) {
-  return 2 * p_stage(mode, fp16) + 16 + kAmpBytes + 16;
-}
-// [stage 0][stage 1][2 mbarriers, queue items][gather products]
-constexpr size_t v_smem(int mode, bool fp16) { return 2 * v_stage(mode, fp16) + 128 + kGatherBytes; }
+constexpr size_t p_smem(int mode, bool fp16) { return 2 * p_stage(mode, fp16) + 16 + kAmpBytes; }
+// The gathers' products (kGatherBytes) reuse the stage buffers after the tiles.
+constexpr size_t v_smem(int mode, bool fp16) { return 2 * v_stage(mode, fp16) + 128; }
+static_assert(2 * kVStage >= kGatherBytes, "gather products fit in the stage buffers");
 
 // Injection at row i1 of a column band: the (coefficient, station) entries
 // of the point in station order, amplitudes of this step staged in `amp`
@@ -108,14 +106,29 @@ __device__ __forceinline__ bool tile_interior(const Grid& g, const TileId& id, i
   return id.r0 >= rlo && id.r0 + TR <= rhi && id.c0 >= clo && id.c0 + TC <= chi;
 }
 
+// The tiles a persistent CTA walks: first, stride, end (exclusive).  With at
+// least one CTA per shot the grid is split into equal groups, one per shot,
+// each walking its shot's tiles round robin, so a CTA sets up one shot only
+// (CTAs left over from the split walk none); otherwise all tiles round robin.
+struct Walk {
+  int t0, stride, end;
+};
+__device__ __forceinline__ Walk tile_walk(int ntiles, int nshots) {
+  const int cps = gridDim.x / nshots;
+  if (cps == 0) return Walk{(int)blockIdx.x, (int)gridDim.x, ntiles};
+  const int sh = blockIdx.x / cps, tps = ntiles / nshots;
+  if (sh >= nshots) return Walk{0, 1, 0};
+  return Walk{sh * tps + (int)blockIdx.x % cps, cps, (sh + 1) * tps};
+}
+
 __device__ __forceinline__ TileId tile_id(const Grid& g, int t) {
   const int nrb = (g.n1e + TR - 1) / TR, ncb = (g.n2e + TC - 1) / TC;
   const int tps = nrb * ncb;
   TileId id;
   id.shot = t / tps;
   const int l = t - id.shot * tps;
-  id.r0 = (l / ncb) * TR;  // row-major: the surface tile row (sources, receivers) first
-  id.c0 = (l % ncb) * TC;
+  id.r0 = (l % nrb) * TR;
+  id.c0 = (l / nrb) * TC;
   return id;
 }
 
@@ -147,7 +160,6 @@ __global__ void __launch_bounds__(kThreadsT, 2)
   extern __shared__ __align__(128) unsigned char smem[];
   uint64_t* bar = reinterpret_cast<uint64_t*>(smem + 2 * kStage);
   float* amp_s = reinterpret_cast<float*>(smem + 2 * kStage + 16);
-  int* item_s = reinterpret_cast<int*>(smem + 2 * kStage + 16 + kAmpBytes);  // tile of each stage
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   if (tid == 0) {
     bar_init(&bar[0]);
@@ -176,19 +188,11 @@ __global__ void __launch_bounds__(kThreadsT, 2)
              l2_evict_first());
     }
   };
-  // Dynamic tile queue: thread 0 takes tiles from the run's counter two ahead
-  // of the one the CTA works on (every CTA takes exactly one index past the
-  // end, so launch it owns counter values (it - first) * (tiles + grid) on).
-  const unsigned qbase = (unsigned)(it - L.first) * (unsigned)(ntiles + gridDim.x);
-  auto take = [&]() { return (int)(atomicAdd(L.qctr, 1u) - qbase); };
-  if (tid == 0) {
-    const int i0 = take();
-    item_s[0] = i0;
-    item_s[1] = i0 < ntiles ? take() : ntiles;
-    if (i0 < ntiles) issue(i0, 0);
-  }
-  __syncthreads();
+  const Walk wk = tile_walk(ntiles, L.nshots);
+  int t = wk.t0;
+  if (tid == 0 && t < wk.end) issue(t, 0);
   uint32_t phase0 = 0, phase1 = 0;
+  int stage = 0;
   const int ld = g.ld, n1e = g.n1e, n2e = g.n2e, npml = g.npml;
   const int off = (MODE == FM_FWD) ? 2 : 3;
   const int hi1 = n1e - off, hi2 = n2e - off;
@@ -205,16 +209,9 @@ __global__ void __launch_bounds__(kThreadsT, 2)
   float inv_vx = 1.f, inv_vz = 1.f, sc_p = 1.f;
   void* hvs = nullptr;
   unsigned lmax = 0;
-  for (int k = 0;; ++k) {
-    const int stage = k & 1;
-    const int t = item_s[stage];
-    if (t >= ntiles) break;
-    const int tn = item_s[stage ^ 1];
-    int pend = ntiles;
-    if (tid == 0 && tn < ntiles) {
-      issue(tn, stage ^ 1);
-      pend = take();
-    }
+  for (; t < wk.end; t += wk.stride) {
+    const int tn = t + wk.stride;
+    if (tid == 0 && tn < wk.end) issue(tn, stage ^ 1);
     const TileId id = tile_id(g, t);
     if (id.shot != cur) {  // CTA-uniform
       if (MODE == FM_STAGE_A && cur >= 0 && live && !flush)
@@ -561,8 +558,8 @@ __global__ void __launch_bounds__(kThreadsT, 2)
         }
       }
     }
-    if (tid == 0) item_s[stage] = pend;
     __syncthreads();  // stage buffer (and staged amplitudes) free for reuse
+    stage ^= 1;
   }
   if (MODE == FM_STAGE_A && cur >= 0 && live && !flush)
     warp_amax_flush(lmax, sd.amax + (size_t)(it - 1) * 3 * kAmaxSlots +
@@ -584,8 +581,7 @@ __global__ void __launch_bounds__(kThreadsT,
   constexpr int kStage = v_stage(MODE, FP16);
   extern __shared__ __align__(128) unsigned char smem[];
   uint64_t* bar = reinterpret_cast<uint64_t*>(smem + 2 * kStage);
-  int* item_s = reinterpret_cast<int*>(smem + 2 * kStage + 16);  // item of each stage
-  float* prod = reinterpret_cast<float*>(smem + 2 * kStage + 128);  // gather products
+  float* prod = reinterpret_cast<float*>(smem);  // gathers run after the tiles
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   if (tid == 0) {
     bar_init(&bar[0]);
@@ -614,21 +610,11 @@ __global__ void __launch_bounds__(kThreadsT,
              &bar[s], pol);
     }
   };
-  // Dynamic queue (counter L.qctr[1]): the receiver / datum gather units
-  // first, then the tiles; thread 0 takes items two ahead (every CTA takes
-  // exactly one index past the end).
-  const int ngb = (MODE == FM_STAGE_A) ? 0 : ngb_per_shot * L.nshots;
-  const int nitems = ngb + ntiles;
-  const unsigned qbase = (unsigned)(it - L.first) * (unsigned)(nitems + gridDim.x);
-  auto take = [&]() { return (int)(atomicAdd(L.qctr + 1, 1u) - qbase); };
-  if (tid == 0) {
-    const int i0 = take();
-    item_s[0] = i0;
-    item_s[1] = i0 < nitems ? take() : nitems;
-    if (i0 >= ngb && i0 < nitems) issue(i0 - ngb, 0);
-  }
-  __syncthreads();
+  const Walk wk = tile_walk(ntiles, L.nshots);
+  int t = wk.t0;
+  if (tid == 0 && t < wk.end) issue(t, 0);
   uint32_t phase0 = 0, phase1 = 0;
+  int stage = 0;
   const int ld = g.ld, n1e = g.n1e, n2e = g.n2e, npml = g.npml;
   const int off = (MODE == FM_FWD) ? 2 : 3;
   const int hi1 = n1e - off, hi2 = n2e - off;
@@ -643,46 +629,9 @@ __global__ void __launch_bounds__(kThreadsT,
   float inv_p = 1.f, sc_vx = 1.f, sc_vz = 1.f;
   void* hps = nullptr;
   unsigned lmx = 0, lmz = 0;
-  // one gather unit: 8 stations of one shot, a warp each, in step it
-  auto gather_unit = [&](int gb) {
-    const int shot = gb / ngb_per_shot;
-    const ShotDevice& so = L.shots[shot];
-    if (!so.active || it > so.nt || so.type_rec != 0) return;
-    const int s = (gb % ngb_per_shot) * 8 + warp;
-    if (s < so.rec.n) {
-      if (so.out) {
-        const float v = warp_gather_ordered(prod + warp * 444, so.rec.ix1, so.rec.ix2,
-                                            so.rec.tile, s, so.p, g.ld, 0, g.n1e, g.n2e);
-        const int row = so.out_reverse ? so.nt - it : it - 1;
-        if (lane == 0) so.out[row + (size_t)so.nt * s] = v;
-      }
-    } else if (s - so.rec.n < so.datum.n && so.red &&
-               (MODE == FM_FWD || MODE == FM_STAGE_B_ES)) {
-      const int d = s - so.rec.n;
-      const float v = warp_gather_ordered(prod + warp * 444, so.datum.ix1, so.datum.ix2,
-                                          so.datum.tile, d,
-                                          so.p + g.npml + (size_t)g.ld * g.npml, g.ld, g.npml,
-                                          g.n1, g.n2);
-      if (lane == 0) so.red[(it - 1) + (size_t)so.nt * d] = v;
-    }
-  };
-  for (int k = 0;; ++k) {
-    const int stage = k & 1;
-    const int item = item_s[stage];
-    if (item >= nitems) break;
-    const int tn = item_s[stage ^ 1];
-    int pend = nitems;
-    if (tid == 0 && tn < nitems) {
-      if (tn >= ngb) issue(tn - ngb, stage ^ 1);
-      pend = take();
-    }
-    if (item < ngb) {  // CTA-uniform
-      gather_unit(item);
-      if (tid == 0) item_s[stage] = pend;
-      __syncthreads();
-      continue;
-    }
-    const int t = item - ngb;
+  for (; t < wk.end; t += wk.stride) {
+    const int tn = t + wk.stride;
+    if (tid == 0 && tn < wk.end) issue(tn, stage ^ 1);
     const TileId id = tile_id(g, t);
     if (id.shot != cur) {
       if (MODE == FM_STAGE_A && cur >= 0 && live) {
@@ -855,13 +804,39 @@ __global__ void __launch_bounds__(kThreadsT,
       stencil_pass(std::true_type{});
     else
       stencil_pass(std::false_type{});
-    if (tid == 0) item_s[stage] = pend;
     __syncthreads();
+    stage ^= 1;
   }
   if (MODE == FM_STAGE_A && cur >= 0 && live) {
     unsigned* a = sd.amax + (size_t)(it - 1) * 3 * kAmaxSlots + ((blockIdx.x * 8 + warp) % kAmaxSlots);
     warp_amax_flush(lmx, a + kAmaxSlots, L.err);
     warp_amax_flush(lmz, a + 2 * kAmaxSlots, L.err);
+  }
+  // receiver / datum gathers (the pressure field is not modified here)
+  if (MODE != FM_STAGE_A) {
+    const int ngb = ngb_per_shot * L.nshots;
+    for (int gb = gridDim.x - 1 - blockIdx.x; gb < ngb; gb += gridDim.x) {
+      const int shot = gb / ngb_per_shot;
+      const ShotDevice& so = L.shots[shot];
+      if (!so.active || it > so.nt || so.type_rec != 0) continue;
+      const int s = (gb % ngb_per_shot) * 8 + warp;
+      if (s < so.rec.n) {
+        if (so.out) {
+          const float v = warp_gather_ordered(prod + warp * 444, so.rec.ix1, so.rec.ix2,
+                                              so.rec.tile, s, so.p, g.ld, 0, g.n1e, g.n2e);
+          const int row = so.out_reverse ? so.nt - it : it - 1;
+          if (lane == 0) so.out[row + (size_t)so.nt * s] = v;
+        }
+      } else if (s - so.rec.n < so.datum.n && so.red &&
+                 (MODE == FM_FWD || MODE == FM_STAGE_B_ES)) {
+        const int d = s - so.rec.n;
+        const float v = warp_gather_ordered(prod + warp * 444, so.datum.ix1, so.datum.ix2,
+                                            so.datum.tile, d,
+                                            so.p + g.npml + (size_t)g.ld * g.npml, g.ld,
+                                            g.npml, g.n1, g.n2);
+        if (lane == 0) so.red[(it - 1) + (size_t)so.nt * d] = v;
+      }
+    }
   }
 }
 
