@@ -371,7 +371,7 @@ def run_ours(args):
     mine = list(range(ista - 1, iend))
     cap = args.batch if args.config == 2 else 8
     h = pkg.Handle(local, preset="mixed", checkpoint=args.checkpoint,
-                   step=1 if args.kernel == "step" else 0, tile_cols=args.tile_cols,
+                   step={"split": 0, "step": 1, "auto": 2}[args.kernel], tile_cols=args.tile_cols,
                    ctas_per_sm=args.ctas_per_sm, pdl=0 if args.no_pdl else 1)
     if args.config == 2:
         per_step = args.batch
@@ -494,7 +494,10 @@ def run_ours(args):
         except Exception as ex:  # the GPU line is still reported
             cpu = {"error": f"{type(ex).__name__}: {ex}"}
     if rank == 0:
-        tc = {m: (tim["tile_cols"][i], tim["ctas_per_sm"][i])
+        tc = {m: {"family": ["p+v kernels", "one kernel per step"][tim["kernel_family"][i]],
+                  "tile": f"64x{tim['tile_cols'][i]}",
+                  "ctas_per_sm": ([tim["ctas_per_sm"][i], tim["ctas_per_sm_v"][i]]
+                                  if tim["kernel_family"][i] == 0 else tim["ctas_per_sm"][i])}
               for i, m in enumerate(("forward", "stage_a", "stage_b", "esource"))}
         result = {
             "metric": METRIC, "value": value, "unit": "shots/hour", "n_gpus": world,
@@ -509,11 +512,13 @@ def run_ours(args):
                        "batching": ("consecutive shots, as many as HBM admits per batch"
                                     if args.config == 4 else f"{args.batch} shots per batch"),
                        "density": "1 (the reference's rho = 1, src/submodeling2.f90:93)",
-                       "kernel": ("one TMA kernel per time step (p recomputed on the v halo)"
-                                  if args.kernel == "step" else
-                                  "TMA pressure and velocity kernels")
+                       "kernel": {"auto": "TMA time-step kernels, family and launch shape "
+                                          "autotuned per mode",
+                                  "split": "TMA pressure and velocity kernels",
+                                  "step": "one TMA kernel per time step (p recomputed on the "
+                                          "v halo)"}[args.kernel]
                                  + ("" if args.no_pdl else ", programmatic dependent launch"),
-                       "autotuned_tile_cols_ctas_per_sm": tc,
+                       "autotuned": tc,
                        "parallelism": f"shots x{world} (para_range, no collective)",
                        "stage_a_history": (f"windows of {args.checkpoint} steps (checkpointed)"
                                            if args.checkpoint > 0 else "whole record"),
@@ -581,7 +586,8 @@ def main():
     ap.add_argument("--maxiter", type=int, default=None)
     ap.add_argument("--no-e2e", action="store_true")
     # A/B: the one-kernel-per-step path (default) or the split p / v kernels
-    ap.add_argument("--kernel", default="split", choices=["step", "split"])
+    # the TMA kernel family: autotuned (default), split p / v kernels, or one per step
+    ap.add_argument("--kernel", default="auto", choices=["auto", "split", "step"])
     ap.add_argument("--no-pdl", action="store_true", help="plain stream order between steps")
     # pin the step kernel's tile width / CTAs per SM (0 = autotuned)
     ap.add_argument("--tile-cols", type=int, default=0, choices=[0, 16, 32])

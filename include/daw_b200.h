@@ -74,10 +74,13 @@ enum daw_option {
                                 from that state while stage B consumes the windows in
                                 reverse order.  No counterpart in the reference, which
                                 keeps whole histories. */,
-  DAW_OPT_STEP_KERNEL = 9,   /* TMA kernels (DAW_OPT_CHUNK = 0): 0 (default) = separate
+  DAW_OPT_STEP_KERNEL = 9,   /* TMA kernel family (DAW_OPT_CHUNK = 0): 0 = separate
                                 pressure and velocity kernels; 1 = one kernel per time
                                 step (pressure recomputed on the velocity stencil's
-                                halo, two alternating state sets) */
+                                halo, two alternating state sets); 2 (default) = chosen
+                                by the autotuner per mode, grid and batch, with the
+                                launch shapes (the windows of a checkpointed shot use
+                                the separate kernels unless 1 is set) */
   DAW_OPT_TILE_COLS = 10,    /* one-kernel-per-step tiles: 16 or 32 columns of 64
                                 rows; 0 (default) = chosen by the autotuner */
   DAW_OPT_CTAS_PER_SM = 11,  /* one-kernel-per-step CTAs per SM (1..3; a value above
@@ -249,9 +252,12 @@ typedef struct daw_timing {
   double hist_bytes;          /* history bytes written + read */
   int64_t kernel_launches;    /* kernels launched by the library */
   double shot_steps_fwd, shot_steps_a, shot_steps_b;  /* shot time steps by kind */
-  /* one-kernel-per-step path: tile columns and CTAs per SM of the last run of
-   * each mode (forward, stage A, stage B, final esource; 0 = not run) */
-  int32_t tile_cols[4], ctas_per_sm[4];
+  /* TMA kernels of the last run of each mode (forward, stage A, stage B, final
+   * esource), as the autotuner chose them: family (0 = separate pressure and
+   * velocity kernels, 1 = one kernel per step), tile columns, CTAs per SM
+   * (separate kernels: of the pressure kernel) and CTAs per SM of the
+   * velocity kernel (0 for one kernel per step); zeros = not run */
+  int32_t kernel_family[4], tile_cols[4], ctas_per_sm[4], ctas_per_sm_v[4];
 } daw_timing;
 int daw_get_timing(const daw_handle* h, daw_timing* t);
 void daw_reset_timing(daw_handle* h);

@@ -221,11 +221,13 @@ struct daw_handle {
   int step_occ[4][2][2] = {};
   unsigned* d_qctr = nullptr;
   struct Tuned {
-    int tile_cols, ctas_per_sm;
-    float us_per_step;
+    int family;            // 0: split pressure / velocity kernels, 1: one kernel per step
+    int tile_cols;         // columns per tile (the split kernels' tiles are 32 wide)
+    int ctas_per_sm;       // CTAs per SM (split: of the pressure kernel)
+    int ctas_per_sm_v;     // split: CTAs per SM of the velocity kernel
+    float us_per_step;     // measured device time of one step (0: not measured)
   };
   std::map<std::string, Tuned> tuned;
-  Tuned last_tuned{0, 0, 0.f};
 };
 
 namespace {
@@ -576,8 +578,15 @@ struct Window {
 // 0: TMA-pipelined persistent kernels (default); 1, 2, 4: register kernels
 // with that many columns per thread.
 int chunk_of(const daw_handle* h) { return h->opt.chunk; }
-// The one-kernel-per-step TMA path (the default of the fused kernels).
-bool step_path(const daw_handle* h) { return h->opt.fused && h->opt.chunk == 0 && h->opt.step; }
+// Tensor maps needed by the TMA kernels: the split kernels' unless the
+// one-kernel-per-step family is pinned, the step kernels' unless the split
+// family is pinned (DAW_OPT_STEP_KERNEL 0 / 1; 2 = autotuned needs both).
+bool tma_path(const daw_handle* h) { return h->opt.fused && h->opt.chunk == 0; }
+bool split_maps(const daw_handle* h) { return tma_path(h) && h->opt.step != 1; }
+bool step_maps(const daw_handle* h) { return tma_path(h) && h->opt.step != 0; }
+// Family of the windows of a checkpointed shot (not tuned): the step kernels
+// only when pinned.
+bool windowed_step(const daw_handle* h) { return tma_path(h) && h->opt.step == 1; }
 
 // Device descriptors (and tensor maps) of the batch's shots for `mode`.  With
 // a window, stage A sees the window as a record of w->len steps whose
@@ -624,7 +633,7 @@ void fill_shot_devices(daw_handle* h, Batch& b, int mode, const Window* w = null
     }
   }
   upload(b.d_shots, b.h_shots.data(), b.h_shots.size() * sizeof(ShotDevice), h->st);
-  if (step_path(h)) {
+  if (step_maps(h)) {
     // tensor maps of every shot for both tile widths: [tile width 16 | 32][shot]
     const size_t n = b.shots.size();
     std::vector<StepMaps> maps(2 * n);
@@ -641,7 +650,8 @@ void fill_shot_devices(daw_handle* h, Batch& b, int mode, const Window* w = null
         maps.size() * sizeof(StepMaps)));
     upload(b.d_smaps, maps.data(), maps.size() * sizeof(StepMaps), h->st);
     sync(h);  // `maps` goes out of scope
-  } else if (chunk_of(h) == 0) {
+  }
+  if (split_maps(h)) {
     // tensor maps of every shot's fields (the TMA kernels' operands)
     std::vector<TmaMaps> maps(b.shots.size());
     for (size_t i = 0; i < b.shots.size(); ++i) {
@@ -701,63 +711,98 @@ void stop_clock(daw_handle* h, SimClock& clk, Batch& b, int mode, const Window* 
   clk.stop(ms, st, w ? w->len : b.max_nt, shot_steps);
 }
 
-// Autotuner of the one-kernel-per-step path: tile width (16 or 32 columns)
-// and CTAs per SM (1 .. occupancy), chosen per (mode, history precision, grid,
-// batch) by timing the run's first step with every candidate (median of 3
-// launches after a warm-up), once per handle.  The first step has no deferred
-// work and writes only the state set it is about to write anyway, and its
-// max-|x| atomics are idempotent, so the trial launches leave no trace; the
-// final esource, whose first step also accumulates into the wavefield output,
-// takes stage B's configuration (same kernel shape) and tunes as stage B.
-daw_handle::Tuned tune_step(daw_handle* h, Batch& b, int mode, FusedLaunch L, int first) {
+// Autotuner of the TMA time-step kernels, per (mode, history precision,
+// grid, batch): the kernel family -- separate pressure and velocity kernels
+// (64 x 32 tiles) with 1 .. occupancy CTAs per SM for each, or one kernel per
+// time step with 16- or 32-column tiles and 1 .. occupancy CTAs per SM -- by
+// timing the run's first step with every candidate (median of 3 launches
+// after a warm-up), once per handle.  Only runs that start from the zero
+// state are tuned (not the windows of a checkpointed shot, which take the
+// family DAW_OPT_STEP_KERNEL names and default launch shapes).  The trials
+// change only what the run itself then overwrites: the first step's state
+// (zeroed again afterwards, and the stage-A max-|x| slots cleared), its
+// history slot and the first rows of the outputs.  The final esource, whose
+// first step also accumulates into the wavefield output, tunes as stage B
+// (same kernel shapes) and takes stage B's choice.
+daw_handle::Tuned tune_run(daw_handle* h, Batch& b, int mode, FusedLaunch L, int first,
+                           bool may_time) {
   const int tmode = mode == FM_STAGE_B_ES ? FM_STAGE_B : mode;
   const int f = L.hist_fp16 ? 1 : 0;
-  char key[160];
-  std::snprintf(key, sizeof key, "m%d.f%d.g%dx%d.p%d.s%d.r%d.d%d.t%d.c%d", tmode, f, h->g.n1,
-                h->g.n2, h->g.npml, L.nshots, L.max_rec, L.max_datum, h->opt.tile_cols,
-                h->opt.ctas_per_sm);
+  const int occ_p = std::max(1, std::min(h->persist_p / h->sms, 3));
+  const int occ_v = std::max(1, std::min(h->persist_v_mode[tmode * 2 + f] / h->sms, 3));
+  std::vector<daw_handle::Tuned> cands;
+  if (h->opt.step != 1)
+    for (int pc = 1; pc <= occ_p; ++pc)
+      for (int vc = 1; vc <= occ_v; ++vc) cands.push_back({0, 32, pc, vc, 0.f});
+  if (h->opt.step != 0)
+    for (int tc : {16, 32}) {
+      if (h->opt.tile_cols && h->opt.tile_cols != tc) continue;
+      // a pinned CTA count above what fits is clamped to the occupancy
+      const int occ = std::min(h->step_occ[tmode][f][tc == 32 ? 1 : 0], 3);
+      const int pin = h->opt.ctas_per_sm ? std::min(h->opt.ctas_per_sm, occ) : 0;
+      for (int c = 1; c <= occ; ++c)
+        if (!pin || pin == c) cands.push_back({1, tc, c, 0, 0.f});
+    }
+  if (cands.empty())
+    throw DawError{DAW_ERR_CUDA, "no resident configuration of the TMA step kernels"};
+  if (!may_time) {  // checkpointed windows: the named family, default shapes
+    for (const auto& c : cands)
+      if (c.family == (h->opt.step == 1 ? 1 : 0) &&
+          (c.family == 0 ? (c.ctas_per_sm == occ_p && c.ctas_per_sm_v == occ_v)
+                         : (c.tile_cols == (h->opt.tile_cols ? h->opt.tile_cols : 32))))
+        return c;
+    return cands.back();
+  }
+  char key[192];
+  std::snprintf(key, sizeof key, "m%d.f%d.g%dx%d.p%d.s%d.r%d.d%d.k%d.t%d.c%d", tmode, f, h->g.n1,
+                h->g.n2, h->g.npml, L.nshots, L.max_rec, L.max_datum, h->opt.step,
+                h->opt.tile_cols, h->opt.ctas_per_sm);
   auto it = h->tuned.find(key);
   if (it != h->tuned.end()) return it->second;
   const size_t n = b.shots.size();
-  std::vector<daw_handle::Tuned> cands;
-  for (int tc : {16, 32}) {
-    if (h->opt.tile_cols && h->opt.tile_cols != tc) continue;
-    // a pinned CTA count above what fits is clamped to the occupancy
-    const int occ = std::min(h->step_occ[tmode][f][tc == 32 ? 1 : 0], 3);
-    const int pin = h->opt.ctas_per_sm ? std::min(h->opt.ctas_per_sm, occ) : 0;
-    for (int c = 1; c <= occ; ++c)
-      if (!pin || pin == c) cands.push_back({tc, c, 0.f});
-  }
-  if (cands.empty())
-    throw DawError{DAW_ERR_CUDA, "no resident configuration of the step kernel"};
   daw_handle::Tuned best = cands[0];
   if (cands.size() > 1) {
     float best_us = 1e30f;
     for (auto& cd : cands) {
       FusedLaunch T = L;
-      T.tile_cols = cd.tile_cols;
-      T.smaps = b.d_smaps + (cd.tile_cols == 32 ? n : 0);
-      const int grid = cd.ctas_per_sm * h->sms;
       float ms[3];
       for (int r = 0; r < 4; ++r) {
-        CK(cudaMemsetAsync(h->d_qctr, 0, sizeof(unsigned), h->st));
+        if (cd.family == 1) CK(cudaMemsetAsync(h->d_qctr, 0, sizeof(unsigned), h->st));
         if (r > 0) CK(cudaEventRecord(h->ev0, h->st));
-        step_launch(h->g, h->md, T, tmode, first, grid, h->st);
+        if (cd.family == 1) {
+          T.tile_cols = cd.tile_cols;
+          T.smaps = b.d_smaps + (cd.tile_cols == 32 ? n : 0);
+          step_launch(h->g, h->md, T, tmode, first, cd.ctas_per_sm * h->sms, h->st);
+        } else {
+          T.persist_p = cd.ctas_per_sm * h->sms;
+          T.persist_v = cd.ctas_per_sm_v * h->sms;
+          tma_p_step(h->g, h->md, T, tmode, first, h->st);
+          tma_v_step(h->g, h->md, T, tmode, first, h->st);
+        }
         if (r > 0) {
           CK(cudaEventRecord(h->ev1, h->st));
           CK(cudaEventSynchronize(h->ev1));
           CK(cudaEventElapsedTime(&ms[r - 1], h->ev0, h->ev1));
         }
       }
-      check_launch("step kernel (tuning)");
+      check_launch("time-step kernels (tuning)");
       std::sort(ms, ms + 3);
       cd.us_per_step = ms[1] * 1e3f;
       if (cd.us_per_step < best_us) {
         best_us = cd.us_per_step;
         best = cd;
       }
+      h->tim.kernel_launches += 4 * (cd.family == 1 ? 1 : 2);
     }
-    h->tim.kernel_launches += 4 * (long long)cands.size();
+    // undo the trials: the run starts from the zero state and clear slots
+    for (ShotCtx* c : b.shots) {
+      if (!c->active) continue;
+      zero_state(h, *c);
+      if (mode == FM_STAGE_A)
+        CK(cudaMemsetAsync(c->amax, 0, (size_t)(c->nt + 1) * 3 * kAmaxSlots * sizeof(unsigned),
+                           h->st));
+    }
+    check_device_error(h);
   }
   h->tuned[key] = best;
   return best;
@@ -803,13 +848,30 @@ void run_fused(daw_handle* h, Batch& b, int mode, const Window* w = nullptr) {
     nt_v = b.max_nt - w->s0;
     L.hist_step0 = w->s0;
   }
-  const bool step = step_path(h);
+  const bool tma = L.chunk == 0;
+  L.first = first;
+  L.step_last = nt_v;
+  L.qctr = h->d_qctr;  // tile queue of the one-kernel-per-step path
+  L.ngath = mode == FM_STAGE_A ? 0 : (L.max_rec + (b.no_datum ? 0 : L.max_datum) + 7) / 8;
+  L.active_mask = 0;
+  for (size_t i = 0; i < b.shots.size() && i < 64; ++i)
+    if (b.shots[i]->active) L.active_mask |= 1ull << i;
+  daw_handle::Tuned tn{0, 32, 0, 0, 0.f};
+  if (tma) {
+    tn = tune_run(h, b, mode, L, first, w == nullptr);
+    h->tim.kernel_family[mode] = tn.family;
+    h->tim.tile_cols[mode] = tn.tile_cols;
+    h->tim.ctas_per_sm[mode] = tn.ctas_per_sm;
+    h->tim.ctas_per_sm_v[mode] = tn.ctas_per_sm_v;
+    if (tn.family == 0) {
+      L.persist_p = tn.ctas_per_sm * h->sms;
+      L.persist_v = tn.ctas_per_sm_v * h->sms;
+    }
+  }
+  const bool step = tma && tn.family == 1;
   // the step path's extra launch does the last step's deferred work; the
   // split kernels' extra stage-A launch flushes its history
   const int last = step ? nt_v + 1 : (mode == FM_STAGE_A) ? nt_v + 1 : nt_v;
-  const bool tma = L.chunk == 0;
-  L.first = first;
-  L.qctr = h->d_qctr;  // tile queue of the one-kernel-per-step path
   int grid = 0;
   if (step) {
     int par0 = -1;
@@ -820,20 +882,9 @@ void run_fused(daw_handle* h, Batch& b, int mode, const Window* w = nullptr) {
       par0 = c->par;
     }
     L.par0 = std::max(par0, 0);
-    L.first = first;
-    L.step_last = nt_v;
-    L.active_mask = 0;
-    for (size_t i = 0; i < b.shots.size() && i < 64; ++i)
-      if (b.shots[i]->active) L.active_mask |= 1ull << i;
-    L.qctr = h->d_qctr;
-    L.ngath = mode == FM_STAGE_A ? 0 : (L.max_rec + (b.no_datum ? 0 : L.max_datum) + 7) / 8;
-    const daw_handle::Tuned t = tune_step(h, b, mode, L, first);
-    h->last_tuned = t;
-    h->tim.tile_cols[mode] = t.tile_cols;
-    h->tim.ctas_per_sm[mode] = t.ctas_per_sm;
-    L.tile_cols = t.tile_cols;
-    L.smaps = b.d_smaps + (t.tile_cols == 32 ? b.shots.size() : 0);
-    grid = t.ctas_per_sm * h->sms;
+    L.tile_cols = tn.tile_cols;
+    L.smaps = b.d_smaps + (tn.tile_cols == 32 ? b.shots.size() : 0);
+    grid = tn.ctas_per_sm * h->sms;
   }
   auto body = [&]() {
     if (step) {
@@ -860,7 +911,8 @@ void run_fused(daw_handle* h, Batch& b, int mode, const Window* w = nullptr) {
                   "m%d.n%d.s%zu.p%p.q%p.z%p.c%d.f%d.r%d.d%d.h%llx.w%d.%d.%d.%d.%d.%d.%d.a%llx.l%d",
                   mode, b.max_nt, b.shots.size(), (void*)b.d_shots, (void*)b.d_maps,
                   (void*)b.d_smaps, L.chunk, L.hist_fp16, L.max_rec, L.max_datum, phash, step,
-                  first, last, L.hist_step0, L.par0, L.tile_cols, grid, L.active_mask, L.pdl);
+                  first, last, L.hist_step0, L.par0, L.tile_cols, grid + 1000 * L.persist_p,
+                  L.active_mask, L.pdl + 2 * L.persist_v);
     auto it = h->graphs.find(key);
     if (it == h->graphs.end()) {
       cudaGraph_t graph;
@@ -933,7 +985,7 @@ void shot_operator_windowed(daw_handle* h, Batch& b, bool esource) {
   const size_t ne = h->g.ext_elems();
   // a saved state: the four fields of the current set (one-kernel-per-step
   // path) or px, pz, vx, vz, p (split kernels); ckpt slots hold 5 fields
-  const bool step = step_path(h);
+  const bool step = windowed_step(h);
   const size_t save_bytes = (step ? 4 : 5) * ne * sizeof(float);
   const int K = c.hist_win, nwin = (c.nt + K - 1) / K;
   float* const st_a = c.state;  // the slot's state block
@@ -1782,7 +1834,11 @@ int daw_set_option(daw_handle* h, int32_t key, double value) {
         if (v < 0) throw DawError{DAW_ERR_ARG, "history window must be >= 0 (0 = automatic)"};
         h->opt.checkpoint = v;
         break;
-      case DAW_OPT_STEP_KERNEL: h->opt.step = v ? 1 : 0; break;
+      case DAW_OPT_STEP_KERNEL:
+        if (v < 0 || v > 2)
+          throw DawError{DAW_ERR_ARG, "step kernel: 0 split, 1 one per step, 2 autotuned"};
+        h->opt.step = v;
+        break;
       case DAW_OPT_PDL: h->opt.pdl = v ? 1 : 0; break;
       case DAW_OPT_TILE_COLS:
         if (v != 0 && v != 16 && v != 32)

@@ -95,7 +95,7 @@ def _handle(pkg, w, preset, **opt):
 PATHS = [("plain", {}), ("mixed", {"history": 0}), ("mixed", {"history": 0, "graph": 0}),
          ("mixed", {"history": 0, "step": 1, "tile_cols": 16}),
          ("mixed", {"history": 0, "step": 1, "tile_cols": 32}),
-         ("mixed", {"history": 0, "pdl": 0}),
+         ("mixed", {"history": 0, "step": 0}), ("mixed", {"history": 0, "pdl": 1}),
          ("mixed", {"history": 0, "chunk": 1}), ("mixed", {"history": 0, "chunk": 2}),
          ("mixed", {"history": 0, "chunk": 4})]
 

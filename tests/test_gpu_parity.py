@@ -36,14 +36,15 @@ def handle(pkg, case, preset="plain", **opt):
     return h
 
 
-# "mixed" with FP32 histories: the split pressure/velocity TMA kernels (the
-# default, with and without programmatic dependent launch), direct launches
-# instead of graphs, the one-kernel-per-step TMA path (both tile widths
-# pinned), and the register kernels.
+# "mixed" with FP32 histories: the TMA kernels with the family and launch
+# shape autotuned (the default), the split pressure/velocity kernels pinned
+# (also with programmatic dependent launch), direct launches instead of
+# graphs, the one-kernel-per-step path (both tile widths pinned), and the
+# register kernels.
 PATHS = [("plain", {}), ("mixed", {"history": 0}), ("mixed", {"history": 0, "graph": 0}),
          ("mixed", {"history": 0, "step": 1, "tile_cols": 16, "ctas_per_sm": 1}),
          ("mixed", {"history": 0, "step": 1, "tile_cols": 32, "ctas_per_sm": 2}),
-         ("mixed", {"history": 0, "pdl": 0}),
+         ("mixed", {"history": 0, "step": 0}), ("mixed", {"history": 0, "pdl": 1}),
          ("mixed", {"history": 0, "chunk": 1}), ("mixed", {"history": 0, "chunk": 4})]
 
 
