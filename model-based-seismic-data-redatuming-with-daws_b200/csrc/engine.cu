@@ -718,14 +718,16 @@ void stop_clock(daw_handle* h, SimClock& clk, Batch& b, int mode, const Window* 
 // timing the run's first step with every candidate (median of 3 launches
 // after a warm-up), once per handle.  Only runs that start from the zero
 // state are tuned (not the windows of a checkpointed shot, which take the
-// family DAW_OPT_STEP_KERNEL names and default launch shapes).  The trials
-// change only what the run itself then overwrites: the first step's state
-// (zeroed again afterwards, and the stage-A max-|x| slots cleared), its
-// history slot and the first rows of the outputs.  The final esource, whose
+// family DAW_OPT_STEP_KERNEL names and default launch shapes).  A trial runs
+// the first two steps, so that the step kernel's work deferred to the next
+// launch (gathers, stage-A history stores) is timed too.  The trials change
+// only what the run itself then overwrites: the state (zeroed again
+// afterwards, and the stage-A max-|x| slots cleared), the first history
+// slots and the first rows of the outputs.  The final esource, whose
 // first step also accumulates into the wavefield output, tunes as stage B
 // (same kernel shapes) and takes stage B's choice.
 daw_handle::Tuned tune_run(daw_handle* h, Batch& b, int mode, FusedLaunch L, int first,
-                           bool may_time) {
+                           int last_step, bool may_time) {
   const int tmode = mode == FM_STAGE_B_ES ? FM_STAGE_B : mode;
   const int f = L.hist_fp16 ? 1 : 0;
   const int occ_p = std::max(1, std::min(h->persist_p / h->sms, 3));
@@ -769,15 +771,19 @@ daw_handle::Tuned tune_run(daw_handle* h, Batch& b, int mode, FusedLaunch L, int
       for (int r = 0; r < 4; ++r) {
         if (cd.family == 1) CK(cudaMemsetAsync(h->d_qctr, 0, sizeof(unsigned), h->st));
         if (r > 0) CK(cudaEventRecord(h->ev0, h->st));
-        if (cd.family == 1) {
-          T.tile_cols = cd.tile_cols;
-          T.smaps = b.d_smaps + (cd.tile_cols == 32 ? n : 0);
-          step_launch(h->g, h->md, T, tmode, first, cd.ctas_per_sm * h->sms, h->st);
-        } else {
-          T.persist_p = cd.ctas_per_sm * h->sms;
-          T.persist_v = cd.ctas_per_sm_v * h->sms;
-          tma_p_step(h->g, h->md, T, tmode, first, h->st);
-          tma_v_step(h->g, h->md, T, tmode, first, h->st);
+        // two steps, so that the step kernel's deferred work of the first
+        // (its gathers, its stage-A history stores) is in the time
+        for (int st = first; st <= std::min(first + 1, last_step); ++st) {
+          if (cd.family == 1) {
+            T.tile_cols = cd.tile_cols;
+            T.smaps = b.d_smaps + (cd.tile_cols == 32 ? n : 0);
+            step_launch(h->g, h->md, T, tmode, st, cd.ctas_per_sm * h->sms, h->st);
+          } else {
+            T.persist_p = cd.ctas_per_sm * h->sms;
+            T.persist_v = cd.ctas_per_sm_v * h->sms;
+            tma_p_step(h->g, h->md, T, tmode, st, h->st);
+            tma_v_step(h->g, h->md, T, tmode, st, h->st);
+          }
         }
         if (r > 0) {
           CK(cudaEventRecord(h->ev1, h->st));
@@ -792,7 +798,7 @@ daw_handle::Tuned tune_run(daw_handle* h, Batch& b, int mode, FusedLaunch L, int
         best_us = cd.us_per_step;
         best = cd;
       }
-      h->tim.kernel_launches += 4 * (cd.family == 1 ? 1 : 2);
+      h->tim.kernel_launches += 8 * (cd.family == 1 ? 1 : 2);
     }
     // undo the trials: the run starts from the zero state and clear slots
     for (ShotCtx* c : b.shots) {
@@ -858,7 +864,7 @@ void run_fused(daw_handle* h, Batch& b, int mode, const Window* w = nullptr) {
     if (b.shots[i]->active) L.active_mask |= 1ull << i;
   daw_handle::Tuned tn{0, 32, 0, 0, 0.f};
   if (tma) {
-    tn = tune_run(h, b, mode, L, first, w == nullptr);
+    tn = tune_run(h, b, mode, L, first, nt_v, w == nullptr);
     h->tim.kernel_family[mode] = tn.family;
     h->tim.tile_cols[mode] = tn.tile_cols;
     h->tim.ctas_per_sm[mode] = tn.ctas_per_sm;
