@@ -862,6 +862,19 @@ void run_fused(daw_handle* h, Batch& b, int mode, const Window* w = nullptr) {
   L.active_mask = 0;
   for (size_t i = 0; i < b.shots.size() && i < 64; ++i)
     if (b.shots[i]->active) L.active_mask |= 1ull << i;
+  // shots with work at step it: active, and it within the record (the split
+  // pressure kernel's stage-A flush step included)
+  auto live_of = [&](FusedLaunch& T, int it, bool velocity) {
+    T.nlive = 0;
+    for (size_t i = 0; i < b.shots.size() && i < 64; ++i) {
+      const ShotCtx* c = b.shots[i];
+      if (!c->active) continue;
+      const int nts = (w && mode == FM_STAGE_A) ? w->len : c->nt;
+      const int lim = nts + ((mode == FM_STAGE_A && !velocity) ? 1 : 0);
+      if (it <= lim) T.live[T.nlive++] = (unsigned char)i;
+    }
+  };
+  live_of(L, first, false);
   daw_handle::Tuned tn{0, 32, 0, 0, 0.f};
   if (tma) {
     tn = tune_run(h, b, mode, L, first, nt_v, w == nullptr);
@@ -900,8 +913,11 @@ void run_fused(daw_handle* h, Batch& b, int mode, const Window* w = nullptr) {
     }
     for (int it = first; it <= last; ++it) {
       if (tma) {
-        tma_p_step(g, h->md, L, mode, it, h->st);
-        if (it <= nt_v) tma_v_step(g, h->md, L, mode, it, h->st);
+        FusedLaunch T = L;
+        live_of(T, it, false);
+        if (T.nlive) tma_p_step(g, h->md, T, mode, it, h->st);
+        live_of(T, it, true);
+        if (it <= nt_v && T.nlive) tma_v_step(g, h->md, T, mode, it, h->st);
       } else {
         fused_p_step(g, h->md, L, mode, it, h->st);
         if (it <= nt_v) fused_v_step(g, h->md, L, mode, it, h->st);
@@ -1630,7 +1646,7 @@ int admit_batch(daw_handle* h, int n, const daw_shot_desc* d, bool want_wf, int*
   *win = history_window(h, d[0].nt, d[0].nrec, want_wf, avail);
   if (*win > 0) return 1;
   const bool fp16 = h->opt.history_fp16 != 0;
-  const int cap = h->opt.max_batch > 0 ? std::min(n, h->opt.max_batch) : n;
+  const int cap = std::min(h->opt.max_batch > 0 ? std::min(n, h->opt.max_batch) : n, 64);
   size_t sum = 0;
   int s = 0;
   while (s < cap) {

@@ -92,6 +92,11 @@ struct FusedLaunch {
   int step_last;  // last stencil step of the run (the extra launch after it does none)
   unsigned long long active_mask;  // bit i: shot i (< 64) takes part in the run
   int pdl;  // TMA kernels launched with programmatic dependent launch
+  // Split TMA kernels: the shots with work in this launch (an uneven batch's
+  // short records end early), live[0 .. nlive-1]; the grid is spread over
+  // them only.
+  int nlive;
+  unsigned char live[64];
   static constexpr int kParamShots = 8;
   int nparam;
   const unsigned* shot_amax[kParamShots];

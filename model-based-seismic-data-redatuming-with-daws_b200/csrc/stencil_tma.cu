@@ -121,12 +121,14 @@ __device__ __forceinline__ Walk tile_walk(int ntiles, int nshots) {
   return Walk{sh * tps + (int)blockIdx.x % cps, cps, (sh + 1) * tps};
 }
 
-__device__ __forceinline__ TileId tile_id(const Grid& g, int t) {
+// Tile t of the launch: group t / tiles-per-shot is live shot L.live[group].
+__device__ __forceinline__ TileId tile_id(const Grid& g, int t, const FusedLaunch& L) {
   const int nrb = (g.n1e + TR - 1) / TR, ncb = (g.n2e + TC - 1) / TC;
   const int tps = nrb * ncb;
   TileId id;
-  id.shot = t / tps;
-  const int l = t - id.shot * tps;
+  const int grp = t / tps;
+  id.shot = L.live[grp];
+  const int l = t - grp * tps;
   id.r0 = (l % nrb) * TR;
   id.c0 = (l / nrb) * TC;
   return id;
@@ -171,7 +173,7 @@ __global__ void __launch_bounds__(kThreadsT, 2)
   pdl_wait();  // the previous step's fields, scales and outputs are complete
   const int hbase = g.hist_base();
   auto issue = [&](int t, int s) {
-    const TileId id = tile_id(g, t);
+    const TileId id = tile_id(g, t, L);
     const TmaMaps* mp = L.maps + id.shot;
     unsigned char* st = smem + s * kStage;
     bar_expect(&bar[s], kStage);  // kPStage (+ history box) = bytes copied
@@ -188,7 +190,7 @@ __global__ void __launch_bounds__(kThreadsT, 2)
              l2_evict_first());
     }
   };
-  const Walk wk = tile_walk(ntiles, L.nshots);
+  const Walk wk = tile_walk(ntiles, L.nlive);
   int t = wk.t0;
   if (tid == 0 && t < wk.end) issue(t, 0);
   uint32_t phase0 = 0, phase1 = 0;
@@ -212,7 +214,7 @@ __global__ void __launch_bounds__(kThreadsT, 2)
   for (; t < wk.end; t += wk.stride) {
     const int tn = t + wk.stride;
     if (tid == 0 && tn < wk.end) issue(tn, stage ^ 1);
-    const TileId id = tile_id(g, t);
+    const TileId id = tile_id(g, t, L);
     if (id.shot != cur) {  // CTA-uniform
       if (MODE == FM_STAGE_A && cur >= 0 && live && !flush)
         warp_amax_flush(lmax, sd.amax + (size_t)(it - 1) * 3 * kAmaxSlots +
@@ -593,7 +595,7 @@ __global__ void __launch_bounds__(kThreadsT,
   pdl_wait();  // the previous step's fields, scales and outputs are complete
   const int hbase = g.hist_base();
   auto issue = [&](int t, int s) {
-    const TileId id = tile_id(g, t);
+    const TileId id = tile_id(g, t, L);
     const TmaMaps* mp = L.maps + id.shot;
     unsigned char* st = smem + s * kStage;
     bar_expect(&bar[s], kVPb + 2 * kPF + (kB ? 2 * hist_box(FP16) : 0));  // bytes copied
@@ -610,7 +612,7 @@ __global__ void __launch_bounds__(kThreadsT,
              &bar[s], pol);
     }
   };
-  const Walk wk = tile_walk(ntiles, L.nshots);
+  const Walk wk = tile_walk(ntiles, L.nlive);
   int t = wk.t0;
   if (tid == 0 && t < wk.end) issue(t, 0);
   uint32_t phase0 = 0, phase1 = 0;
@@ -632,7 +634,7 @@ __global__ void __launch_bounds__(kThreadsT,
   for (; t < wk.end; t += wk.stride) {
     const int tn = t + wk.stride;
     if (tid == 0 && tn < wk.end) issue(tn, stage ^ 1);
-    const TileId id = tile_id(g, t);
+    const TileId id = tile_id(g, t, L);
     if (id.shot != cur) {
       if (MODE == FM_STAGE_A && cur >= 0 && live) {
         unsigned* a = sd.amax + (size_t)(it - 1) * 3 * kAmaxSlots + ((blockIdx.x * 8 + warp) % kAmaxSlots);
@@ -814,9 +816,9 @@ __global__ void __launch_bounds__(kThreadsT,
   }
   // receiver / datum gathers (the pressure field is not modified here)
   if (MODE != FM_STAGE_A) {
-    const int ngb = ngb_per_shot * L.nshots;
+    const int ngb = ngb_per_shot * L.nlive;
     for (int gb = gridDim.x - 1 - blockIdx.x; gb < ngb; gb += gridDim.x) {
-      const int shot = gb / ngb_per_shot;
+      const int shot = L.live[gb / ngb_per_shot];
       const ShotDevice& so = L.shots[shot];
       if (!so.active || it > so.nt || so.type_rec != 0) continue;
       const int s = (gb % ngb_per_shot) * 8 + warp;
@@ -842,7 +844,7 @@ __global__ void __launch_bounds__(kThreadsT,
 
 template <int MODE>
 void launch_p(const Grid& g, const ModelDev& m, const FusedLaunch& L, int it, cudaStream_t st) {
-  const int ntiles = tma_tiles(g) * L.nshots;
+  const int ntiles = tma_tiles(g) * L.nlive;
   const int grid = std::min(ntiles, L.persist_p);
   if (L.hist_fp16)
     launch_pdl(k_tma_p<MODE, true>, grid, kThreadsT, p_smem(MODE, true), st, L.pdl != 0, g, m, L,
@@ -854,10 +856,10 @@ void launch_p(const Grid& g, const ModelDev& m, const FusedLaunch& L, int it, cu
 
 template <int MODE>
 void launch_v(const Grid& g, const ModelDev& m, const FusedLaunch& L, int it, cudaStream_t st) {
-  const int ntiles = tma_tiles(g) * L.nshots;
+  const int ntiles = tma_tiles(g) * L.nlive;
   const int stations = (MODE == FM_STAGE_A) ? 0 : L.max_rec + L.max_datum;
   const int ngbps = (stations + 7) / 8;
-  const int grid = std::max(1, std::min(std::max(ntiles, ngbps * L.nshots), L.persist_v));
+  const int grid = std::max(1, std::min(std::max(ntiles, ngbps * L.nlive), L.persist_v));
   if (L.hist_fp16)
     launch_pdl(k_tma_v<MODE, true>, grid, kThreadsT, v_smem(MODE, true), st, L.pdl != 0, g, m, L,
                it, ntiles, ngbps);

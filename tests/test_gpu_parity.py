@@ -335,3 +335,34 @@ def test_batched_forward_matches_single(pkg, O, case, preset):
             ora, _ = O.submodeling(w.c0, w.npml, w.h, w.ofs, sh["nt"], w.dt, sh["s"], sh["src"],
                                    sh["rec"])
             assert np.array_equal(g1, ora)
+
+
+@pytest.mark.parametrize("opt", [{}, {"step": 0}, {"step": 1}])
+def test_batched_eleven_uneven_shots(pkg, O, case, opt):
+    """Eleven shots in one batch -- more than the 8 whose per-shot pointers
+    travel as kernel parameters, so the rest take the descriptor-load path --
+    with record lengths 250..400 and receiver spreads of 7..24 channels; the
+    short records end early, so later steps run on a subset of the batch.
+    Every output equals the same shots run one per batch, bit for bit."""
+    w = case["w"]
+    rng = np.random.default_rng(11)
+    shots = []
+    for k in range(11):
+        nt = int(rng.integers(250, 401))
+        lo = int(rng.integers(0, 12))
+        hi = int(rng.integers(lo + 7, 25))
+        x = float(rng.uniform(200.0, 700.0))
+        src = pkg.subacqui([[15.0, x]], w.h, w.npml, w.ofs)[0]
+        rec = case["rec"][lo:hi]
+        s = w.wavelet(nt)
+        dobs, _ = O.submodeling(w.vtrue, w.npml, w.h, w.ofs, nt, w.dt, s, src, rec)
+        shots.append(dict(s=s, nt=nt, src=src, rec=rec, dobs=dobs, mu=w.mu, maxiter=2,
+                          rtol=0.0, band=w.band, shot=k + 1))
+    with handle(pkg, case, "mixed", **opt) as h:
+        h.set_datum(case["ird"])
+        batched = h.shots(shots)
+        h.set_options(max_batch=1)
+        serial = h.shots(shots)
+    for b, s1 in zip(batched, serial):
+        for key in ("datar", "deltadr", "deltade", "dataesc", "redatumed"):
+            assert np.array_equal(b[key], s1[key]), key
