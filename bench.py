@@ -497,7 +497,8 @@ def run_ours(args):
         tc = {m: {"family": ["p+v kernels", "one kernel per step"][tim["kernel_family"][i]],
                   "tile": f"64x{tim['tile_cols'][i]}",
                   "ctas_per_sm": ([tim["ctas_per_sm"][i], tim["ctas_per_sm_v"][i]]
-                                  if tim["kernel_family"][i] == 0 else tim["ctas_per_sm"][i])}
+                                  if tim["kernel_family"][i] == 0 else tim["ctas_per_sm"][i]),
+                  "shots_per_launch": tim["shots_per_launch"][i]}
               for i, m in enumerate(("forward", "stage_a", "stage_b", "esource"))}
         result = {
             "metric": METRIC, "value": value, "unit": "shots/hour", "n_gpus": world,
@@ -514,7 +515,8 @@ def run_ours(args):
                        "density": "1 (the reference's rho = 1, src/submodeling2.f90:93)",
                        "kernel": {"auto": "TMA time-step kernels, family and launch shape "
                                           "autotuned per mode",
-                                  "split": "TMA pressure and velocity kernels",
+                                  "split": "TMA pressure and velocity kernels, shots per launch "
+                                           "and CTAs per SM autotuned per mode",
                                   "step": "one TMA kernel per time step (p recomputed on the "
                                           "v halo)"}[args.kernel]
                                  + ("" if args.no_pdl else ", programmatic dependent launch"),
@@ -587,7 +589,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     # A/B: the one-kernel-per-step path (default) or the split p / v kernels
     # the TMA kernel family: autotuned (default), split p / v kernels, or one per step
-    ap.add_argument("--kernel", default="auto", choices=["auto", "split", "step"])
+    ap.add_argument("--kernel", default="split", choices=["split", "step", "auto"])
     ap.add_argument("--no-pdl", action="store_true", help="plain stream order between steps")
     # pin the step kernel's tile width / CTAs per SM (0 = autotuned)
     ap.add_argument("--tile-cols", type=int, default=0, choices=[0, 16, 32])

@@ -74,13 +74,14 @@ enum daw_option {
                                 from that state while stage B consumes the windows in
                                 reverse order.  No counterpart in the reference, which
                                 keeps whole histories. */,
-  DAW_OPT_STEP_KERNEL = 9,   /* TMA kernel family (DAW_OPT_CHUNK = 0): 0 = separate
-                                pressure and velocity kernels; 1 = one kernel per time
-                                step (pressure recomputed on the velocity stencil's
-                                halo, two alternating state sets); 2 (default) = chosen
-                                by the autotuner per mode, grid and batch, with the
-                                launch shapes (the windows of a checkpointed shot use
-                                the separate kernels unless 1 is set) */
+  DAW_OPT_STEP_KERNEL = 9,   /* TMA kernel family (DAW_OPT_CHUNK = 0): 0 (default) =
+                                separate pressure and velocity kernels, shots per launch
+                                and CTAs per SM chosen by the autotuner; 1 = one kernel
+                                per time step (pressure recomputed on the velocity
+                                stencil's halo, two alternating state sets), tile width
+                                and CTAs per SM autotuned; 2 = the family autotuned too
+                                (the windows of a checkpointed shot use the separate
+                                kernels unless 1 is set) */
   DAW_OPT_TILE_COLS = 10,    /* one-kernel-per-step tiles: 16 or 32 columns of 64
                                 rows; 0 (default) = chosen by the autotuner */
   DAW_OPT_CTAS_PER_SM = 11,  /* one-kernel-per-step CTAs per SM (1..3; a value above
@@ -258,6 +259,7 @@ typedef struct daw_timing {
    * (separate kernels: of the pressure kernel) and CTAs per SM of the
    * velocity kernel (0 for one kernel per step); zeros = not run */
   int32_t kernel_family[4], tile_cols[4], ctas_per_sm[4], ctas_per_sm_v[4];
+  int32_t shots_per_launch[4]; /* shots whose time loops share one launch */
 } daw_timing;
 int daw_get_timing(const daw_handle* h, daw_timing* t);
 void daw_reset_timing(daw_handle* h);

@@ -78,7 +78,8 @@ class Timing(C.Structure):
                 ("kernel_launches", C.c_int64), ("shot_steps_fwd", C.c_double),
                 ("shot_steps_a", C.c_double), ("shot_steps_b", C.c_double),
                 ("kernel_family", C.c_int32 * 4), ("tile_cols", C.c_int32 * 4),
-                ("ctas_per_sm", C.c_int32 * 4), ("ctas_per_sm_v", C.c_int32 * 4)]
+                ("ctas_per_sm", C.c_int32 * 4), ("ctas_per_sm_v", C.c_int32 * 4),
+                ("shots_per_launch", C.c_int32 * 4)]
 
 
 _lib = None

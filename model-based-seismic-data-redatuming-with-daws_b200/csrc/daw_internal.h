@@ -121,7 +121,7 @@ struct Options {
   int max_batch = 0;
   int chunk = 0;
   int checkpoint = 0;  // stage-A history window in steps (0 = automatic)
-  int step = 2;        // TMA kernels: 0 = p and v kernels, 1 = one kernel per step, 2 = autotuned
+  int step = 0;        // TMA kernels: 0 = p and v kernels, 1 = one kernel per step, 2 = autotuned
   int pdl = 0;         // TMA kernels: programmatic dependent launch between time steps
   int tile_cols = 0;   // one-kernel-per-step tiles: 16 or 32 columns, 0 = autotuned
   int ctas_per_sm = 0; // one-kernel-per-step CTAs per SM, 0 = autotuned

@@ -225,7 +225,9 @@ struct daw_handle {
     int tile_cols;         // columns per tile (the split kernels' tiles are 32 wide)
     int ctas_per_sm;       // CTAs per SM (split: of the pressure kernel)
     int ctas_per_sm_v;     // split: CTAs per SM of the velocity kernel
-    float us_per_step;     // measured device time of one step (0: not measured)
+    int sub;               // split: shots per launch (the batch's time loops run in
+                           // groups of `sub` shots); 0 = the whole batch
+    float us_per_step;     // measured device time of one step per shot (0: not measured)
   };
   std::map<std::string, Tuned> tuned;
 };
@@ -700,42 +702,125 @@ void check_device_error(daw_handle* h) {
   }
 }
 
-void stop_clock(daw_handle* h, SimClock& clk, Batch& b, int mode, const Window* w) {
+void stop_clock(daw_handle* h, SimClock& clk, Batch& b, int mode, const Window* w, int lo = 0,
+                int hi = -1) {
+  if (hi < 0) hi = (int)b.shots.size();
   double shot_steps = 0;
-  for (ShotCtx* c : b.shots)
+  int gmax = 0;
+  for (int i = lo; i < hi; ++i) {
+    const ShotCtx* c = b.shots[i];
     if (c->active) shot_steps += w ? w->len : c->nt;
+    gmax = std::max(gmax, c->nt);
+  }
   double* ms = mode == FM_FWD ? &h->tim.sim_fwd_ms : mode == FM_STAGE_A ? &h->tim.sim_a_ms : &h->tim.sim_b_ms;
   double* st = mode == FM_FWD ? &h->tim.steps_fwd : mode == FM_STAGE_A ? &h->tim.steps_a : &h->tim.steps_b;
   (mode == FM_FWD ? h->tim.shot_steps_fwd : mode == FM_STAGE_A ? h->tim.shot_steps_a
                                                                 : h->tim.shot_steps_b) += shot_steps;
-  clk.stop(ms, st, w ? w->len : b.max_nt, shot_steps);
+  clk.stop(ms, st, w ? w->len : gmax, shot_steps);
 }
 
 // Autotuner of the TMA time-step kernels, per (mode, history precision,
-// grid, batch): the kernel family -- separate pressure and velocity kernels
-// (64 x 32 tiles) with 1 .. occupancy CTAs per SM for each, or one kernel per
-// time step with 16- or 32-column tiles and 1 .. occupancy CTAs per SM -- by
-// timing the run's first step with every candidate (median of 3 launches
-// after a warm-up), once per handle.  Only runs that start from the zero
-// state are tuned (not the windows of a checkpointed shot, which take the
-// family DAW_OPT_STEP_KERNEL names and default launch shapes).  A trial runs
-// the first two steps, so that the step kernel's work deferred to the next
-// launch (gathers, stage-A history stores) is timed too.  The trials change
-// only what the run itself then overwrites: the state (zeroed again
-// afterwards, and the stage-A max-|x| slots cleared), the first history
-// slots and the first rows of the outputs.  The final esource, whose
-// first step also accumulates into the wavefield output, tunes as stage B
-// (same kernel shapes) and takes stage B's choice.
+// grid, batch).  Candidates are timed over the run's first two steps (so the
+// one-kernel-per-step family's work deferred to the next launch is counted),
+// median of 3 after a warm-up, and compared by device time per shot step:
+//   - separate pressure and velocity kernels (64 x 32 tiles): the shots per
+//     launch -- an HBM-admitted batch can run its time loops in groups of k
+//     shots, and the fastest k is often below the batch because the groups'
+//     wavefield state then stays in L2 -- and then, for that k, 1 ..
+//     occupancy CTAs per SM of each kernel;
+//   - with DAW_OPT_STEP_KERNEL = 2 or 1, one kernel per step with 16- or
+//     32-column tiles and 1 .. occupancy CTAs per SM (whole batch).
+// Only runs that start from the zero state are tuned; the windows of a
+// checkpointed shot take the family DAW_OPT_STEP_KERNEL names with default
+// shapes.  The trials change only what the run itself then overwrites: the
+// state (zeroed again afterwards, and the stage-A max-|x| slots cleared), the
+// first history slots and the first rows of the outputs.  The final esource,
+// whose first step also accumulates into the wavefield output, tunes as stage
+// B (same kernel shapes) and takes stage B's choice.
 daw_handle::Tuned tune_run(daw_handle* h, Batch& b, int mode, FusedLaunch L, int first,
                            int last_step, bool may_time) {
   const int tmode = mode == FM_STAGE_B_ES ? FM_STAGE_B : mode;
   const int f = L.hist_fp16 ? 1 : 0;
   const int occ_p = std::max(1, std::min(h->persist_p / h->sms, 3));
   const int occ_v = std::max(1, std::min(h->persist_v_mode[tmode * 2 + f] / h->sms, 3));
-  std::vector<daw_handle::Tuned> cands;
-  if (h->opt.step != 1)
-    for (int pc = 1; pc <= occ_p; ++pc)
-      for (int vc = 1; vc <= occ_v; ++vc) cands.push_back({0, 32, pc, vc, 0.f});
+  std::vector<int> act;  // active shots (indices < 64)
+  for (size_t i = 0; i < b.shots.size() && i < 64; ++i)
+    if (b.shots[i]->active) act.push_back((int)i);
+  const int nact = std::max<int>(1, (int)act.size());
+  const daw_handle::Tuned split_default{0, 32, occ_p, occ_v, 0, 0.f};
+  if (!may_time) {  // checkpointed windows: the named family, default shapes
+    if (h->opt.step == 1) {
+      const int tc = h->opt.tile_cols ? h->opt.tile_cols : 32;
+      const int occ = std::max(1, std::min(h->step_occ[tmode][f][tc == 32 ? 1 : 0], 3));
+      return {1, tc, h->opt.ctas_per_sm ? std::min(h->opt.ctas_per_sm, occ) : occ, 0, 0, 0.f};
+    }
+    return split_default;
+  }
+  char key[192];
+  std::snprintf(key, sizeof key, "m%d.f%d.g%dx%d.p%d.s%d.a%d.r%d.d%d.k%d.t%d.c%d", tmode, f,
+                h->g.n1, h->g.n2, h->g.npml, L.nshots, nact, L.max_rec, L.max_datum,
+                h->opt.step, h->opt.tile_cols, h->opt.ctas_per_sm);
+  auto found = h->tuned.find(key);
+  if (found != h->tuned.end()) return found->second;
+  const size_t n = b.shots.size();
+  auto trial = [&](const daw_handle::Tuned& cd) -> float {  // us per shot step
+    FusedLaunch T = L;
+    const int k = cd.family == 0 && cd.sub > 0 ? std::min(cd.sub, nact) : nact;
+    if (cd.family == 0) {
+      T.nlive = 0;
+      for (int i = 0; i < k && i < (int)act.size(); ++i) T.live[T.nlive++] = (unsigned char)act[i];
+      T.persist_p = cd.ctas_per_sm * h->sms;
+      T.persist_v = cd.ctas_per_sm_v * h->sms;
+    } else {
+      T.tile_cols = cd.tile_cols;
+      T.smaps = b.d_smaps + (cd.tile_cols == 32 ? n : 0);
+    }
+    const int nst = std::min(first + 1, last_step) - first + 1;
+    float ms[3];
+    for (int r = 0; r < 4; ++r) {
+      if (cd.family == 1) CK(cudaMemsetAsync(h->d_qctr, 0, sizeof(unsigned), h->st));
+      if (r > 0) CK(cudaEventRecord(h->ev0, h->st));
+      for (int st = first; st < first + nst; ++st) {
+        if (cd.family == 1) {
+          step_launch(h->g, h->md, T, tmode, st, cd.ctas_per_sm * h->sms, h->st);
+        } else {
+          tma_p_step(h->g, h->md, T, tmode, st, h->st);
+          tma_v_step(h->g, h->md, T, tmode, st, h->st);
+        }
+      }
+      if (r > 0) {
+        CK(cudaEventRecord(h->ev1, h->st));
+        CK(cudaEventSynchronize(h->ev1));
+        CK(cudaEventElapsedTime(&ms[r - 1], h->ev0, h->ev1));
+      }
+    }
+    check_launch("time-step kernels (tuning)");
+    h->tim.kernel_launches += 4 * nst * (cd.family == 1 ? 1 : 2);
+    std::sort(ms, ms + 3);
+    return ms[1] * 1e3f / (float)(nst * k);
+  };
+  daw_handle::Tuned best = split_default;
+  best.us_per_step = 1e30f;
+  bool timed = false;
+  auto consider = [&](daw_handle::Tuned cd) {
+    cd.us_per_step = trial(cd);
+    timed = true;
+    if (cd.us_per_step < best.us_per_step) best = cd;
+  };
+  if (h->opt.step != 1) {
+    // shots per launch (default shapes), then the CTAs per SM for the best
+    std::vector<int> ks;
+    for (int k : {1, 2, 3, 4, 6, 8, 12, 16, 24, 32, 48, 64})
+      if (k < nact) ks.push_back(k);
+    ks.push_back(nact);
+    if (ks.size() > 1)
+      for (int k : ks) consider({0, 32, occ_p, occ_v, k == nact ? 0 : k, 0.f});
+    const int kbest = best.family == 0 ? best.sub : 0;
+    if (occ_p * occ_v > 1)
+      for (int pc = 1; pc <= occ_p; ++pc)
+        for (int vc = 1; vc <= occ_v; ++vc)
+          if (!(timed && pc == occ_p && vc == occ_v)) consider({0, 32, pc, vc, kbest, 0.f});
+  }
   if (h->opt.step != 0)
     for (int tc : {16, 32}) {
       if (h->opt.tile_cols && h->opt.tile_cols != tc) continue;
@@ -743,63 +828,10 @@ daw_handle::Tuned tune_run(daw_handle* h, Batch& b, int mode, FusedLaunch L, int
       const int occ = std::min(h->step_occ[tmode][f][tc == 32 ? 1 : 0], 3);
       const int pin = h->opt.ctas_per_sm ? std::min(h->opt.ctas_per_sm, occ) : 0;
       for (int c = 1; c <= occ; ++c)
-        if (!pin || pin == c) cands.push_back({1, tc, c, 0, 0.f});
+        if (!pin || pin == c) consider({1, tc, c, 0, 0, 0.f});
     }
-  if (cands.empty())
-    throw DawError{DAW_ERR_CUDA, "no resident configuration of the TMA step kernels"};
-  if (!may_time) {  // checkpointed windows: the named family, default shapes
-    for (const auto& c : cands)
-      if (c.family == (h->opt.step == 1 ? 1 : 0) &&
-          (c.family == 0 ? (c.ctas_per_sm == occ_p && c.ctas_per_sm_v == occ_v)
-                         : (c.tile_cols == (h->opt.tile_cols ? h->opt.tile_cols : 32))))
-        return c;
-    return cands.back();
-  }
-  char key[192];
-  std::snprintf(key, sizeof key, "m%d.f%d.g%dx%d.p%d.s%d.r%d.d%d.k%d.t%d.c%d", tmode, f, h->g.n1,
-                h->g.n2, h->g.npml, L.nshots, L.max_rec, L.max_datum, h->opt.step,
-                h->opt.tile_cols, h->opt.ctas_per_sm);
-  auto it = h->tuned.find(key);
-  if (it != h->tuned.end()) return it->second;
-  const size_t n = b.shots.size();
-  daw_handle::Tuned best = cands[0];
-  if (cands.size() > 1) {
-    float best_us = 1e30f;
-    for (auto& cd : cands) {
-      FusedLaunch T = L;
-      float ms[3];
-      for (int r = 0; r < 4; ++r) {
-        if (cd.family == 1) CK(cudaMemsetAsync(h->d_qctr, 0, sizeof(unsigned), h->st));
-        if (r > 0) CK(cudaEventRecord(h->ev0, h->st));
-        // two steps, so that the step kernel's deferred work of the first
-        // (its gathers, its stage-A history stores) is in the time
-        for (int st = first; st <= std::min(first + 1, last_step); ++st) {
-          if (cd.family == 1) {
-            T.tile_cols = cd.tile_cols;
-            T.smaps = b.d_smaps + (cd.tile_cols == 32 ? n : 0);
-            step_launch(h->g, h->md, T, tmode, st, cd.ctas_per_sm * h->sms, h->st);
-          } else {
-            T.persist_p = cd.ctas_per_sm * h->sms;
-            T.persist_v = cd.ctas_per_sm_v * h->sms;
-            tma_p_step(h->g, h->md, T, tmode, st, h->st);
-            tma_v_step(h->g, h->md, T, tmode, st, h->st);
-          }
-        }
-        if (r > 0) {
-          CK(cudaEventRecord(h->ev1, h->st));
-          CK(cudaEventSynchronize(h->ev1));
-          CK(cudaEventElapsedTime(&ms[r - 1], h->ev0, h->ev1));
-        }
-      }
-      check_launch("time-step kernels (tuning)");
-      std::sort(ms, ms + 3);
-      cd.us_per_step = ms[1] * 1e3f;
-      if (cd.us_per_step < best_us) {
-        best_us = cd.us_per_step;
-        best = cd;
-      }
-      h->tim.kernel_launches += 8 * (cd.family == 1 ? 1 : 2);
-    }
+  if (!timed) best = split_default;
+  if (timed) {
     // undo the trials: the run starts from the zero state and clear slots
     for (ShotCtx* c : b.shots) {
       if (!c->active) continue;
@@ -864,9 +896,9 @@ void run_fused(daw_handle* h, Batch& b, int mode, const Window* w = nullptr) {
     if (b.shots[i]->active) L.active_mask |= 1ull << i;
   // shots with work at step it: active, and it within the record (the split
   // pressure kernel's stage-A flush step included)
-  auto live_of = [&](FusedLaunch& T, int it, bool velocity) {
+  auto live_of = [&](FusedLaunch& T, int it, bool velocity, int lo = 0, int hi = 64) {
     T.nlive = 0;
-    for (size_t i = 0; i < b.shots.size() && i < 64; ++i) {
+    for (size_t i = lo; i < b.shots.size() && (int)i < std::min(hi, 64); ++i) {
       const ShotCtx* c = b.shots[i];
       if (!c->active) continue;
       const int nts = (w && mode == FM_STAGE_A) ? w->len : c->nt;
@@ -875,13 +907,14 @@ void run_fused(daw_handle* h, Batch& b, int mode, const Window* w = nullptr) {
     }
   };
   live_of(L, first, false);
-  daw_handle::Tuned tn{0, 32, 0, 0, 0.f};
+  daw_handle::Tuned tn{0, 32, 0, 0, 0, 0.f};
   if (tma) {
     tn = tune_run(h, b, mode, L, first, nt_v, w == nullptr);
     h->tim.kernel_family[mode] = tn.family;
     h->tim.tile_cols[mode] = tn.tile_cols;
     h->tim.ctas_per_sm[mode] = tn.ctas_per_sm;
     h->tim.ctas_per_sm_v[mode] = tn.ctas_per_sm_v;
+    h->tim.shots_per_launch[mode] = tn.family == 0 && tn.sub ? tn.sub : (int)b.shots.size();
     if (tn.family == 0) {
       L.persist_p = tn.ctas_per_sm * h->sms;
       L.persist_v = tn.ctas_per_sm_v * h->sms;
@@ -905,54 +938,65 @@ void run_fused(daw_handle* h, Batch& b, int mode, const Window* w = nullptr) {
     L.smaps = b.d_smaps + (tn.tile_cols == 32 ? b.shots.size() : 0);
     grid = tn.ctas_per_sm * h->sms;
   }
-  auto body = [&]() {
-    if (step) {
-      CK(cudaMemsetAsync(h->d_qctr, 0, sizeof(unsigned), h->st));
-      for (int it = first; it <= last; ++it) step_launch(g, h->md, L, mode, it, grid, h->st);
-      return;
-    }
-    for (int it = first; it <= last; ++it) {
-      if (tma) {
-        FusedLaunch T = L;
-        live_of(T, it, false);
-        if (T.nlive) tma_p_step(g, h->md, T, mode, it, h->st);
-        live_of(T, it, true);
-        if (it <= nt_v && T.nlive) tma_v_step(g, h->md, T, mode, it, h->st);
-      } else {
-        fused_p_step(g, h->md, L, mode, it, h->st);
-        if (it <= nt_v) fused_v_step(g, h->md, L, mode, it, h->st);
+  // The time loop of shots [lo, hi) of the batch (the split kernels run an
+  // admitted batch in groups of the tuned shots per launch; the other paths
+  // take the whole batch).
+  auto run_group = [&](int lo, int hi) {
+    auto body = [&]() {
+      if (step) {
+        CK(cudaMemsetAsync(h->d_qctr, 0, sizeof(unsigned), h->st));
+        for (int it = first; it <= last; ++it) step_launch(g, h->md, L, mode, it, grid, h->st);
+        return;
       }
+      for (int it = first; it <= last; ++it) {
+        if (tma) {
+          FusedLaunch T = L;
+          live_of(T, it, false, lo, hi);
+          if (T.nlive) tma_p_step(g, h->md, T, mode, it, h->st);
+          live_of(T, it, true, lo, hi);
+          if (it <= nt_v && T.nlive) tma_v_step(g, h->md, T, mode, it, h->st);
+        } else {
+          fused_p_step(g, h->md, L, mode, it, h->st);
+          if (it <= nt_v) fused_v_step(g, h->md, L, mode, it, h->st);
+        }
+      }
+    };
+    if (h->opt.graph) {
+      char key[360];
+      std::snprintf(key, sizeof key,
+                    "m%d.n%d.s%zu.p%p.q%p.z%p.c%d.f%d.r%d.d%d.h%llx.w%d.%d.%d.%d.%d.%d.%d.a%llx.l%d"
+                    ".g%d.%d.v%d",
+                    mode, b.max_nt, b.shots.size(), (void*)b.d_shots, (void*)b.d_maps,
+                    (void*)b.d_smaps, L.chunk, L.hist_fp16, L.max_rec, L.max_datum, phash, step,
+                    first, last, L.hist_step0, L.par0, L.tile_cols, grid, L.active_mask, L.pdl,
+                    lo, hi, L.persist_p * 1000 + L.persist_v);
+      auto it = h->graphs.find(key);
+      if (it == h->graphs.end()) {
+        cudaGraph_t graph;
+        CK(cudaStreamBeginCapture(h->st, cudaStreamCaptureModeThreadLocal));
+        body();
+        CK(cudaStreamEndCapture(h->st, &graph));
+        cudaGraphExec_t exec;
+        CK(cudaGraphInstantiate(&exec, graph, 0));
+        cudaGraphDestroy(graph);
+        it = h->graphs.emplace(key, exec).first;
+      }
+      SimClock clk(h);
+      CK(cudaGraphLaunch(it->second, h->st));
+      stop_clock(h, clk, b, mode, w, lo, hi);
+    } else {
+      SimClock clk(h);
+      body();
+      stop_clock(h, clk, b, mode, w, lo, hi);
     }
   };
   const int nsteps = nt_v - first + 1;
-  const long long launches = step ? (long long)nsteps + 1
-                                  : 2LL * nsteps + (mode == FM_STAGE_A ? 1 : 0);
-  if (h->opt.graph) {
-    char key[320];
-    std::snprintf(key, sizeof key,
-                  "m%d.n%d.s%zu.p%p.q%p.z%p.c%d.f%d.r%d.d%d.h%llx.w%d.%d.%d.%d.%d.%d.%d.a%llx.l%d",
-                  mode, b.max_nt, b.shots.size(), (void*)b.d_shots, (void*)b.d_maps,
-                  (void*)b.d_smaps, L.chunk, L.hist_fp16, L.max_rec, L.max_datum, phash, step,
-                  first, last, L.hist_step0, L.par0, L.tile_cols, grid + 1000 * L.persist_p,
-                  L.active_mask, L.pdl + 2 * L.persist_v);
-    auto it = h->graphs.find(key);
-    if (it == h->graphs.end()) {
-      cudaGraph_t graph;
-      CK(cudaStreamBeginCapture(h->st, cudaStreamCaptureModeThreadLocal));
-      body();
-      CK(cudaStreamEndCapture(h->st, &graph));
-      cudaGraphExec_t exec;
-      CK(cudaGraphInstantiate(&exec, graph, 0));
-      cudaGraphDestroy(graph);
-      it = h->graphs.emplace(key, exec).first;
-    }
-    SimClock clk(h);
-    CK(cudaGraphLaunch(it->second, h->st));
-    stop_clock(h, clk, b, mode, w);
-  } else {
-    SimClock clk(h);
-    body();
-    stop_clock(h, clk, b, mode, w);
+  long long launches = 0;
+  const int nb = (int)b.shots.size();
+  const int k = (tma && !step && tn.sub > 0) ? tn.sub : nb;
+  for (int lo = 0; lo < nb; lo += k) {
+    run_group(lo, std::min(nb, lo + k));
+    launches += step ? (long long)nsteps + 1 : 2LL * nsteps + (mode == FM_STAGE_A ? 1 : 0);
   }
   check_launch("fused steps");
   check_device_error(h);
