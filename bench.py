@@ -380,7 +380,20 @@ def run_ours(args):
         need = min(len(mine), 4 * (args.warmup + args.steps))
     ids = [mine[i % len(mine)] for i in range(need)]
     shots = shot_dicts(pkg, h, w, ids, model_dobs=not reduced)
-    # steps: consecutive admitted batches (config 2: the same batch each step)
+    # config 4: batches of similar record lengths (the shots sorted by nt,
+    # each batch as many as HBM admits, as daw_shots forms them), run in a
+    # seeded shuffled order so the warm-up and timed steps draw a
+    # representative mix of the set's record lengths; config 2: the same
+    # batch each step
+    batches = []
+    if args.config == 4:
+        srt = sorted(shots, key=lambda sh: -sh["nt"])
+        i = 0
+        while i < len(srt):
+            k = stage_batch(pkg, h, srt, i, cap)
+            batches.append(srt[i:i + k])
+            i += k
+        np.random.default_rng(4).shuffle(batches)
     pos = 0
     dev_ms, step_shots = [], []
     first_batch = None
@@ -393,12 +406,11 @@ def run_ours(args):
                 pos = 1
             k = len(shots)
         else:
-            if pos >= len(shots):
-                pos = 0
-            k = stage_batch(pkg, h, shots, pos, cap)
+            bt = batches[pos % len(batches)]
+            k = stage_batch(pkg, h, bt, 0, len(bt))
             if timed and first_batch is None:
-                first_batch = shots[pos:pos + k]
-            pos += k
+                first_batch = bt[:k]
+            pos += 1
         ms = h.run_staged()
         if timed:
             dev_ms.append(ms)
@@ -510,7 +522,8 @@ def run_ours(args):
             "config": {"workload": workload_text(w, args),
                        "shots_per_step": [int(x) for x in step_shots],
                        "shots_timed": int(shots_done),
-                       "batching": ("consecutive shots, as many as HBM admits per batch"
+                       "batching": ("shots sorted by record length, as many per batch as HBM "
+                                    "admits, batches in seeded shuffled order"
                                     if args.config == 4 else f"{args.batch} shots per batch"),
                        "density": "1 (the reference's rho = 1, src/submodeling2.f90:93)",
                        "kernel": {"auto": "TMA time-step kernels, family and launch shape "

@@ -216,10 +216,10 @@ typedef struct daw_shot_out {   /* every pointer may be NULL */
 int daw_shot(daw_handle* h, const daw_shot_desc* desc, daw_shot_out* out);
 
 /* Batched: n shots (uneven nt, receiver spreads and sources allowed) run in
- * shared launches.  Batches are formed in order: each takes the longest run
- * of the remaining shots whose device bytes (each shot's own record length
- * and receiver count) fit ~92 % of the free HBM.  outs[i] pairs with
- * descs[i]. */
+ * shared launches.  The shots are taken longest record first (so a batch
+ * holds similar record lengths); each batch takes the longest run of the
+ * remaining shots whose device bytes (each shot's own record length and
+ * receiver count) fit ~92 % of the free HBM.  outs[i] pairs with descs[i]. */
 int daw_shots(daw_handle* h, int32_t n, const daw_shot_desc* descs, daw_shot_out* outs);
 
 /* Batched forward modelling, mode 0 (sub_redatum_DAW.f90:55-72: submodeling

@@ -1714,25 +1714,35 @@ void release_slots(daw_handle* h) {
   for (const char* p : {"slot", "shot", "mr", "batch."}) h->pool.release_prefix(p);
 }
 
+// Shots run longest record first, so that the shots of a batch (and of its
+// launch groups) have similar record lengths and few time steps run with
+// part of a batch idle; outputs go to their own descriptors' slots.
 void run_shots(daw_handle* h, int n, const daw_shot_desc* descs, daw_shot_out* outs) {
   require_model(h);
   if (n <= 0) return;
   bool want_wf = false;
   for (int i = 0; i < n; ++i) want_wf |= (outs && outs[i].wavefield_exd != nullptr);
+  std::vector<int> order(n);
+  for (int i = 0; i < n; ++i) order[i] = i;
+  std::stable_sort(order.begin(), order.end(),
+                   [&](int a, int b) { return descs[a].nt > descs[b].nt; });
+  std::vector<daw_shot_desc> sorted(n);
+  for (int i = 0; i < n; ++i) sorted[i] = descs[order[i]];
   for (int first = 0; first < n;) {
     release_slots(h);
     int win = 0;
-    const int cnt = admit_batch(h, n - first, descs + first, want_wf, &win);
+    const int cnt = admit_batch(h, n - first, sorted.data() + first, want_wf, &win);
     std::vector<ShotCtx> ctx(cnt);
     Batch b;
     b.slot0 = 0;
     for (int i = 0; i < cnt; ++i) {
-      prepare_shot(h, ctx[i], descs[first + i], i, outs && outs[first + i].wavefield_exd,
+      const int o = order[first + i];
+      prepare_shot(h, ctx[i], descs[o], i, outs && outs[o].wavefield_exd,
                    h->opt.history_fp16 != 0, false, win);
       b.shots.push_back(&ctx[i]);
     }
     run_pipeline(h, b);
-    for (int i = 0; i < cnt; ++i) fetch_outputs(h, ctx[i], outs ? &outs[first + i] : nullptr);
+    for (int i = 0; i < cnt; ++i) fetch_outputs(h, ctx[i], outs ? &outs[order[first + i]] : nullptr);
     drop_graphs(h);
     first += cnt;
   }
