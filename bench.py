@@ -390,7 +390,7 @@ def run_ours(args):
         srt = sorted(shots, key=lambda sh: -sh["nt"])
         i = 0
         while i < len(srt):
-            k = stage_batch(pkg, h, srt, i, cap)
+            k = min(h.admit_shots(srt[i:i + cap])[0], cap)
             batches.append(srt[i:i + k])
             i += k
         np.random.default_rng(4).shuffle(batches)

@@ -231,6 +231,13 @@ int daw_shots(daw_handle* h, int32_t n, const daw_shot_desc* descs, daw_shot_out
 int daw_submodeling_shots(daw_handle* h, int32_t n, const daw_shot_desc* descs,
                           float* const* sis);
 
+/* Batch planning (no counterpart in the reference; no device work): *count
+ * receives how many of descs[0 .. n-1], taken in order, HBM admits as one
+ * batch (the rule of daw_shots), *window (nullable) the stage-A history
+ * window a lone shot would use (0 = whole record). */
+int daw_admit_shots(daw_handle* h, int32_t n, const daw_shot_desc* descs, int32_t* count,
+                    int32_t* window);
+
 /* Device-resident timing support: shots whose inputs were staged once with
  * daw_stage_shots run with no host transfers; results stay on the device
  * until daw_fetch_shots. ms_out (nullable) receives the device time. */

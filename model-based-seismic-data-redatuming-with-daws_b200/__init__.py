@@ -121,6 +121,7 @@ def _declare(L):
     L.daw_shots.argtypes = [vp, i32, C.POINTER(ShotDesc), C.POINTER(ShotOut)]
     L.daw_submodeling_shots.argtypes = [vp, i32, C.POINTER(ShotDesc), C.POINTER(fp)]
     L.daw_stage_shots.argtypes = [vp, i32, C.POINTER(ShotDesc)]
+    L.daw_admit_shots.argtypes = [vp, i32, C.POINTER(ShotDesc), ip, ip]
     L.daw_run_staged.argtypes = [vp, fp]
     L.daw_fetch_shots.argtypes = [vp, C.POINTER(ShotOut)]
     L.daw_run_parfile.argtypes = [vp, C.c_char_p, i32, i32]
@@ -350,6 +351,15 @@ class Handle:
 
     def shot(self, **shot):
         return self.shots([shot])[0]
+
+    def admit_shots(self, shots):
+        """(count, window): how many of `shots`, in order, HBM admits as one
+        batch, and the history window a lone shot would use."""
+        descs, _, keep, _ = _pack(shots, (), False, self.grid)
+        cnt, win = C.c_int32(), C.c_int32()
+        self._ck(lib().daw_admit_shots(self._h, len(shots), descs, C.byref(cnt), C.byref(win)))
+        del keep
+        return cnt.value, win.value
 
     def stage_shots(self, shots):
         descs, _, keep, _ = _pack(shots, (), False, self.grid)

@@ -2241,6 +2241,17 @@ void daw_reset_timing(daw_handle* h) {
 // Device-resident runs: inputs copied once into pinned-free host copies, then
 // uploaded to the device by daw_stage_shots' first batch; daw_run_staged runs
 // the whole pipeline with no host<->device traffic of shot data.
+int daw_admit_shots(daw_handle* h, int32_t n, const daw_shot_desc* descs, int32_t* count,
+                    int32_t* window) {
+  return guarded(h, [&] {
+    require_model(h);
+    if (n <= 0 || !descs || !count) throw DawError{DAW_ERR_ARG, "daw_admit_shots: bad arguments"};
+    int win = 0;
+    *count = admit_batch(h, n, descs, false, &win);
+    if (window) *window = win;
+  });
+}
+
 int daw_stage_shots(daw_handle* h, int32_t n, const daw_shot_desc* descs) {
   return guarded(h, [&] {
     require_model(h);
