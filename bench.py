@@ -53,9 +53,9 @@ sys.path.insert(0, ROOT)
 import __graft_entry__ as entry  # noqa: E402
 
 PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
-# DRAM bytes per shot time step of the step kernels, measured by ncu on the
-# same grid
-TRAFFIC = os.path.join(ROOT, "profiles", "k_step_751x2301_traffic.json")
+# DRAM bytes per shot time step of the pressure + velocity kernels, measured
+# by ncu on the same grid
+TRAFFIC = os.path.join(ROOT, "profiles", "k_tma_751x2301_traffic.json")
 METRIC = "shots/hour redatumed at <=1e-3 rel err vs FP64: batched mixed vs plain FP32"
 
 
