@@ -79,12 +79,21 @@ def make_workload(config=4, nt=None):
     if config == 4:
         w = synthetic.config3(3, nshot=256)
         w.name = "cfg4"
+    elif config == 5:
+        w = synthetic.config5()
+        w.nt = nt or 1000
+        w.nts = [w.nt] * len(w.nts)
     else:
         w = synthetic.config2(2, nshot=50, nt=nt or 7500)
     return w
 
 
 def workload_text(w, args):
+    if w.name == "cfg5":
+        return (f"2001x8001 h=5 m, npml 50, nt {w.nt} @ 0.4 ms (reduced from 10000), 1200 "
+                f"receivers, 20 Hz, {w.maxiter} MINRES iterations (reduced from 30), datum at "
+                f"2500 m, FP16 histories / FP64 MINRES scalars; a reduced variant, not the "
+                f"benchmark")
     if w.name == "cfg4":
         return ("751x2301 h=4 m, npml 40, 256 shots with nt U[3000,7500] @ 0.4 ms and 100-576 "
                 "receivers (seeded split offsets), 15 Hz, 20 MINRES iterations, datum at 1200 m, "
@@ -353,6 +362,38 @@ def reference_runs(pkg, local, shots, base_out):
     return res
 
 
+def cfg5_checks(pkg, h, w, shots, args):
+    """2001x8001: the history window HBM admission picks for one full
+    10000-step shot, and, on the reduced shot, the whole-record outputs
+    against windows of nt/4 steps (equal bit for bit by construction)."""
+    ne = (w.n1 + 2 * w.npml) * (w.n2 + 2 * w.npml)
+    n1h = ((w.npml - (w.npml & ~7)) + w.n1 + 7) // 8 * 8
+    hist_step = 3 * n1h * w.n2 * 2
+    full = dict(shots[0])
+    full.update(nt=10000, s=w.wavelet(10000),
+                dobs=np.zeros((10000, full["rec"].shape[0]), np.float32, order="F"))
+    _, win_full = h.admit_shots([full])
+    out = {"history_bytes_per_step_fp16": hist_step,
+           "whole_history_bytes_nt10000": hist_step * 10000,
+           "state_bytes": 5 * ne * 4,
+           "auto_window_nt10000": win_full,
+           "auto_windows_nt10000": -(-10000 // win_full) if win_full else 1}
+    k = max(1, w.nt // 4)
+    outs = {}
+    for name, ck in (("whole", 0), ("windows", k)):
+        h.set_options(checkpoint=ck)
+        h.stage_shots(shots[:1])
+        h.reset_timing()
+        ms = h.run_staged()
+        outs[name] = h.fetch_staged(outputs=("deltade", "redatumed"))[0]
+        out[f"{name}_ms"] = ms
+    h.set_options(checkpoint=args.checkpoint)
+    out["window_checked"] = k
+    out["windows_vs_whole_rel_l2"] = {
+        key: rel(outs["windows"][key], outs["whole"][key]) for key in ("deltade", "redatumed")}
+    return out
+
+
 def run_ours(args):
     pkg = entry.load_package()
     from daw_b200 import ranks
@@ -362,8 +403,12 @@ def run_ours(args):
     if args.maxiter is not None:
         w.maxiter = args.maxiter
     reduced = args.config == 2 and (w.nt != 7500 or w.maxiter != 20)
+    if args.config == 5 and args.maxiter is None:
+        w.maxiter = 2
+    # variants (reduced records, the 2001x8001 grid) skip the CPU arms
+    variant = reduced or args.config == 5
     cfg1 = None
-    if rank == 0 and world == 1 and not reduced and not args.no_accuracy:
+    if rank == 0 and world == 1 and not variant and not args.no_accuracy:
         cfg1 = Cfg1Oracle(pkg)  # CPU threads overlap the GPU timing
     # this rank's shots (para_range of the shot set), cycled when a run needs more
     nsh = len(w.src_pos)
@@ -373,13 +418,14 @@ def run_ours(args):
     h = pkg.Handle(local, preset="mixed", checkpoint=args.checkpoint,
                    step={"split": 0, "step": 1, "auto": 2}[args.kernel], tile_cols=args.tile_cols,
                    ctas_per_sm=args.ctas_per_sm, pdl=0 if args.no_pdl else 1)
-    if args.config == 2:
+    if args.config in (2, 5):
         per_step = args.batch
         need = per_step
     else:
         need = min(len(mine), 4 * (args.warmup + args.steps))
     ids = [mine[i % len(mine)] for i in range(need)]
     shots = shot_dicts(pkg, h, w, ids, model_dobs=not reduced)
+    cfg5 = cfg5_checks(pkg, h, w, shots, args) if args.config == 5 else None
     # config 4: batches of similar record lengths (the shots sorted by nt,
     # each batch as many as HBM admits, as daw_shots forms them), run in a
     # seeded shuffled order so the warm-up and timed steps draw a
@@ -402,7 +448,7 @@ def run_ours(args):
 
     def one_step(timed):
         nonlocal pos, first_batch
-        if args.config == 2:
+        if args.config in (2, 5):
             if pos == 0:
                 stage_batch(pkg, h, shots, 0, cap)
                 pos = 1
@@ -423,7 +469,7 @@ def run_ours(args):
 
     for _ in range(args.warmup):
         one_step(False)
-    if args.config == 2:
+    if args.config in (2, 5):
         first_batch = shots
     h.reset_timing()
     ranks.barrier(dist)
@@ -510,7 +556,7 @@ def run_ours(args):
         cfg1_full = {"seconds": t32, "ns_per_update": t32 / cfg1_upd * 1e9,
                      "note": "one whole 151x461 shot (nt 2000, 10 iterations) of the FP32 CPU "
                              "restatement, one thread, timed while the GPU bench ran"}
-    if rank == 0 and world == 1 and not args.no_cpu and not reduced:
+    if rank == 0 and world == 1 and not args.no_cpu and not variant:
         print(json.dumps({"partial": True, "value": value, "e2e": e2e, "plain_fp32": plain}),
               file=sys.stderr, flush=True)
         try:
@@ -561,6 +607,7 @@ def run_ours(args):
             "fused_fp32": fused,
             "accuracy": acc,
             "cpu_baseline": cpu,
+            "cfg5": cfg5,
             "timing_ms": {k: tim[k] for k in ("forward_ms", "operator_ms", "minres_vec_ms",
                                               "esource_ms", "filter_ms")},
         }
@@ -601,8 +648,9 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", type=int, default=4, choices=[2, 4])
-    ap.add_argument("--batch", type=int, default=2, help="--config 2: shots per batch")
+    ap.add_argument("--config", type=int, default=4, choices=[2, 4, 5])
+    ap.add_argument("--batch", type=int, default=None,
+                    help="--config 2 / 5: shots per batch (default 2 / 1)")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-accuracy", action="store_true")
@@ -624,10 +672,14 @@ def main():
     # stage-A history in windows of K steps (checkpointed; one shot per launch)
     ap.add_argument("--checkpoint", type=int, default=0)
     args = ap.parse_args()
-    if args.checkpoint > 0 and (args.batch != 1 or args.config != 2):
+    if args.batch is None:
+        args.batch = 1 if args.config == 5 else 2
+    if args.config == 5 and args.nt == 7500:
+        args.nt = 1000
+    if args.checkpoint > 0 and (args.batch != 1 or args.config == 4):
         ap.error("--checkpoint runs one shot per launch: give --config 2 --batch 1")
-    if (args.nt != 7500 or args.maxiter is not None) and args.config != 2:
-        ap.error("--nt / --maxiter are profiling variants of --config 2")
+    if (args.nt != 7500 or args.maxiter is not None) and args.config == 4:
+        ap.error("--nt / --maxiter are profiling variants of --config 2 and 5")
     if args.impl == "reference":
         run_reference(args)
     else:

@@ -150,3 +150,29 @@ def test_requested_window_too_small_is_refused(pkg, case):
         h.set_options(checkpoint=3000)
         g = h.submodeling_adjoint_esource_data(np.zeros((300, 4), np.float32, order="F"), rec)
         assert not g.any()
+
+
+def test_windowed_equals_whole_record_on_2001x8001(pkg):
+    """The 2001 x 8001 grid (h = 5 m, npml 50, 1200 receivers, datum at
+    2500 m) with a short record: a shot with stage-A history windows of 30
+    steps equals the whole-record shot bit for bit (two MINRES iterations)."""
+    from daw_b200 import synthetic
+    w = synthetic.config5()
+    nt = 90
+    src = pkg.subacqui(w.src_pos[512:513], w.h, w.npml, w.ofs)[0]
+    rec = pkg.subacqui(w.rec_pos[0][::8], w.h, w.npml, w.ofs)
+    ird = pkg.subacqui(w.datum_pos[::8], w.h, w.npml, w.ofs)
+    s = w.wavelet(nt + 60)[60:].copy()
+    with pkg.Handle(0, preset="mixed") as h:
+        h.set_model(w.vtrue, w.npml, w.h, w.dt, w.ofs)
+        dobs, _ = h.submodeling(s, src, rec)
+        h.set_model(w.c0, w.npml, w.h, w.dt, w.ofs)
+        h.set_datum(ird)
+        kw = dict(s=s, nt=nt, src=src, rec=rec, dobs=dobs, mu=w.mu, maxiter=2, rtol=0.0,
+                  band=w.band)
+        whole = h.shot(**kw)
+        h.set_options(checkpoint=30)
+        win = h.shot(**kw)
+    assert np.abs(whole["deltade"]).max() > 0
+    for key in ("datar", "deltade", "dataesc", "redatumed"):
+        assert np.array_equal(win[key], whole[key]), key
