@@ -424,7 +424,9 @@ def run_ours(args):
     else:
         need = min(len(mine), 4 * (args.warmup + args.steps))
     ids = [mine[i % len(mine)] for i in range(need)]
-    shots = shot_dicts(pkg, h, w, ids, model_dobs=not reduced)
+    # reduced records end before a reflection separates the true and
+    # background models: observed data zero (residual = -datar) there
+    shots = shot_dicts(pkg, h, w, ids, model_dobs=not variant)
     cfg5 = cfg5_checks(pkg, h, w, shots, args) if args.config == 5 else None
     # config 4: batches of similar record lengths (the shots sorted by nt,
     # each batch as many as HBM admits, as daw_shots forms them), run in a
