@@ -161,7 +161,7 @@ def test_windowed_equals_whole_record_on_2001x8001(pkg):
     from daw_b200 import synthetic
     w = synthetic.config5()
     nt = 90
-    src = pkg.subacqui(w.src_pos[512:513], w.h, w.npml, w.ofs)[0]
+    src = pkg.subacqui(w.src_pos[100:101], w.h, w.npml, w.ofs)[0]  # x = 3900 m, a receiver below
     rec = pkg.subacqui(w.rec_pos[0][::8], w.h, w.npml, w.ofs)
     ird = pkg.subacqui(w.datum_pos[::8], w.h, w.npml, w.ofs)
     s = w.wavelet(nt + 60)[60:].copy()
