@@ -171,3 +171,47 @@ def test_parfile_wavefield_files_and_modes_2_3(pkg, case, tmp_path):
         for i in range(2):
             red, _ = h.filmartin2d(h.subwavefieldresample(wexd3[i], rec), w.dt, *w.band)
             assert np.array_equal(_read(f("dataobs_redatum_", i), (nt, nr)), red)
+
+
+@pytest.mark.parametrize("preset,prec,tol", [("plain", "f32", 1e-4), ("mixed", "f64", 1e-3)])
+def test_parfile_mode3_against_oracle(pkg, O, case, tmp_path, preset, prec, tol):
+    """Mode 3 (the Symes variant, sub_redatum_DAW.f90:157-228) against the
+    CPU oracle: the time-reversed observed data are the residual
+    (:174-178), MINRES solves for deltade (:192), and the final extended
+    source gives dataesc and the wavefield (:208-219).  The plain FP32 port is
+    held to the FP32 oracle (1e-4), the mixed path to the FP64 oracle (1e-3);
+    deltadr is a reversal, bit for bit."""
+    w = case["w"]
+    d = str(tmp_path)
+    src_pos = np.array([w.src_pos[0]], np.float32)
+    rec_pos = np.asarray(w.rec_pos[0], np.float32)
+    hh = np.float32(w.h) * np.float32(w.h)
+    s_file = (case["s"] * hh).astype(np.float32)
+    s_api = (s_file / hh).astype(np.float32)
+    _raw(os.path.join(d, "vtrue.bin"), w.vtrue)
+    _raw(os.path.join(d, "vinit.bin"), w.c0)
+    _raw(os.path.join(d, "wavelet.bin"), s_file)
+    _acqui(os.path.join(d, "acqui.txt"), src_pos, rec_pos)
+    rec = O.acqui_table(rec_pos, w.h, w.npml, w.ofs)
+    src = O.acqui_table(src_pos, w.h, w.npml, w.ofs)[0]
+    nt, nr = w.nt, rec.shape[0]
+    dobs, _ = O.submodeling(w.vtrue, w.npml, w.h, w.ofs, nt, w.dt, s_api, src, rec)
+    _raw(os.path.join(d, "dataobs_org_00001.bin"), dobs)
+    _par(os.path.join(d, "redatum.par"), w, 3, 3, oio=1)
+    with pkg.Handle(0, preset=preset) as h:
+        h.run_parfile(d)
+    f = lambda name: os.path.join(d, f"{name}00001.bin")
+    T = np.float32 if prec == "f32" else np.float64
+    deltadr = np.asfortranarray(dobs[::-1]).astype(T)
+    ref_de, info = O.linear_minres(w.c0, w.npml, w.h, w.ofs, nt, w.dt, rec, deltadr, w.mu, 3,
+                                   0.0, prec=prec)
+    assert info["itn"] == 3
+    ref_esc, ref_wf, _ = O.esource(w.c0, w.npml, w.h, w.ofs, nt, w.dt, ref_de, rec, prec=prec)
+    from conftest import rel_l2
+    assert np.array_equal(_read(f("deltadr_"), (nt, nr)), dobs)
+    got_de = _read(f("deltade_"), (nt, nr))[::-1]
+    assert rel_l2(got_de, ref_de) <= tol, rel_l2(got_de, ref_de)
+    got_esc = _read(f("dataesc_"), (nt, nr))
+    assert rel_l2(got_esc, ref_esc) <= tol, rel_l2(got_esc, ref_esc)
+    got_wf = _read(f("wavefield_exd"), (w.n1, w.n2, nt))
+    assert rel_l2(got_wf, ref_wf) <= tol, rel_l2(got_wf, ref_wf)
