@@ -349,13 +349,20 @@ def reference_runs(pkg, local, shots, base_out):
             h.set_model(*base_out["model"])
             h.set_datum(base_out["datum"])
             ms, outs, launches, i = 0.0, [], 0, 0
-            while i < len(shots):
-                k = stage_batch(pkg, h, shots, i, len(shots))
-                h.reset_timing()
-                ms += h.run_staged()
-                launches += h.timing()["kernel_launches"]
-                outs += h.fetch_staged(outputs=("deltade", "redatumed"))
-                i += k
+            try:
+                while i < len(shots):
+                    k = stage_batch(pkg, h, shots, i, len(shots))
+                    h.reset_timing()
+                    ms += h.run_staged()
+                    launches += h.timing()["kernel_launches"]
+                    outs += h.fetch_staged(outputs=("deltade", "redatumed"))
+                    i += k
+            except pkg.DawError as e:
+                if e.code != -2:
+                    raise
+                # the plain port keeps whole FP32 histories (no windows)
+                res[name] = {"unavailable": f"does not fit the GPU: {e}", "outs": None}
+                continue
             res[name] = {"value": len(shots) * 3600.0 / (ms * 1e-3), "unit": "shots/hour",
                          "ms": ms, "shots": len(shots), "kernel_launches": int(launches),
                          "outs": outs}
@@ -530,11 +537,13 @@ def run_ours(args):
         mixed_same = None
         if args.config == 4:
             mixed_same = len(first_batch) * 3600.0 / (dev_ms[0] * 1e-3)
-        plain["ratio_mixed_over_plain"] = (mixed_same or per_shot_value) / plain["value"]
+        if "value" in plain:
+            plain["ratio_mixed_over_plain"] = (mixed_same or per_shot_value) / plain["value"]
+            plain["mixed_vs_plain_rel_l2"] = {
+                "redatumed": max(rel(a["redatumed"], b["redatumed"])
+                                 for a, b in zip(mixed_first, outp)),
+                "deltade": max(rel(a["deltade"], b["deltade"]) for a, b in zip(mixed_first, outp))}
         fused["ratio_mixed_over_fused_fp32"] = (mixed_same or per_shot_value) / fused["value"]
-        plain["mixed_vs_plain_rel_l2"] = {
-            "redatumed": max(rel(a["redatumed"], b["redatumed"]) for a, b in zip(mixed_first, outp)),
-            "deltade": max(rel(a["deltade"], b["deltade"]) for a, b in zip(mixed_first, outp))}
         acc = {"batch_mixed_vs_fp32_history": {
             "shots": [sh["shot"] for sh in first_batch],
             "redatumed": max(rel(a["redatumed"], b["redatumed"]) for a, b in zip(mixed_first, out32)),
