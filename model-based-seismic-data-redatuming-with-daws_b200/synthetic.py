@@ -113,8 +113,12 @@ def config2(seed: int = 2, nshot: int = 50, nt: int = 7500) -> Workload:
 
 
 def config3(seed: int = 3, nshot: int = 256) -> Workload:
-    """cfg2 model, 256 shots, nt ~ U[3000,7500], spreads of 100-576 channels."""
+    """cfg2 model, 256 shots, nt ~ U[3000,7500], spreads of 100-576 channels.
+    The sources are spread evenly over the model (100 m .. 9100 m at z = 8 m):
+    the 180 m spacing of the 50-shot set would run off the 9.2 km model."""
     base = config2(2, nshot=nshot)
+    base.src_pos = np.stack([np.full(nshot, 8.0), np.linspace(100.0, 9100.0, nshot)],
+                            1).astype(np.float32)
     rng = np.random.default_rng(seed)
     nts = rng.integers(3000, 7501, nshot).tolist()
     recs = []
