@@ -12,6 +12,8 @@
 #include <string>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "daw_internal.h"
 #include "fused.cuh"
 #include "kernels.cuh"
@@ -1551,7 +1553,14 @@ void run_forward_shots(daw_handle* h, int n, const daw_shot_desc* descs, float* 
   }
 }
 
+// An NVTX range around a scope (a pipeline phase), shown by nsys / ncu.
+struct NvtxRange {
+  explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+};
+
 void run_pipeline(daw_handle* h, Batch& b) {
+  NvtxRange batch_range("daw shot batch");
   cudaStream_t st = h->st;
   cudaEvent_t e0, e1;
   CK(cudaEventCreate(&e0));
@@ -1570,21 +1579,26 @@ void run_pipeline(daw_handle* h, Batch& b) {
         h->pool.get("batch.shots" + std::to_string(b.slot0), b.shots.size() * sizeof(ShotDevice)));
   }
   // 1. forward modelling in c0 (sub_redatum_DAW.f90:82)
+  nvtxRangePushA("daw forward");
   CK(cudaEventRecord(e0, st));
   batch_forward(h, b);
   CK(cudaEventRecord(e1, st));
   CK(cudaEventSynchronize(e1));
   CK(cudaEventElapsedTime(&ms, e0, e1));
   h->tim.forward_ms += ms;
+  nvtxRangePop();
   // 2. time-reversed residuals (:103)
   for (ShotCtx* c : b.shots) residuals(c->d_dobs, c->d_datar, c->d_deltadr, c->nt, c->nr, st);
   check_launch("residuals");
   // 3. MINRES (:115)
+  nvtxRangePushA("daw minres");
   if (h->opt.scalars_fp64)
     batch_minres<double>(h, b);
   else
     batch_minres<float>(h, b);
+  nvtxRangePop();
   // 4. final extended-source simulation (:131) with the datum gather
+  nvtxRangePushA("daw esource");
   for (ShotCtx* c : b.shots) {
     c->active = true;
     c->op_in = c->d_deltade;
@@ -1598,7 +1612,9 @@ void run_pipeline(daw_handle* h, Batch& b) {
   CK(cudaEventSynchronize(e1));
   CK(cudaEventElapsedTime(&ms, e0, e1));
   h->tim.esource_ms += ms;
+  nvtxRangePop();
   // 5. DAW data and the redatumed data at the datum (:143-145, :238-240)
+  nvtxRangePushA("daw datum and filter");
   CK(cudaEventRecord(e0, st));
   for (ShotCtx* c : b.shots) {
     vec_add(c->d_datar, c->d_dataesc, c->d_datae, (size_t)c->nt * c->nr, st);
@@ -1611,6 +1627,7 @@ void run_pipeline(daw_handle* h, Batch& b) {
   CK(cudaEventSynchronize(e1));
   CK(cudaEventElapsedTime(&ms, e0, e1));
   h->tim.filter_ms += ms;
+  nvtxRangePop();
   for (ShotCtx* c : b.shots) download(&c->cost, c->d_cost, sizeof(double), st);
   sync(h);
   cudaEventDestroy(e0);
