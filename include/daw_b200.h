@@ -106,6 +106,20 @@ int daw_get_option(const daw_handle* h, int32_t key, double* value);
 int daw_set_model(daw_handle* h, const float* vp, int32_t n1, int32_t n2, int32_t npml,
                   float hgrid, float dt, int32_t ofs);
 
+/* The same with a density rho(n1,n2) (column-major; NULL = rho 1, the same
+ * as daw_set_model).  The reference allocates rho and fixes it to 1
+ * (submodeling2.f90:88-93, :961); this entry point passes a real density
+ * through its substagger arithmetic (:1227-1270): kappa = rho vp^2 in double,
+ * buoyancy 1/rho (1e10 where rho <= 0) averaged onto the staggered velocity
+ * grids, and the buoyancy weight of the velocity sources (:252, :838, :845).
+ * A density other than 1 runs on the plain kernels and the split TMA
+ * pressure/velocity kernels; the register kernels (DAW_OPT_CHUNK != 0) and
+ * the one-kernel-per-step family (DAW_OPT_STEP_KERNEL = 1) refuse it with
+ * DAW_ERR_ARG, and the autotuner (DAW_OPT_STEP_KERNEL = 2) keeps to the
+ * split kernels. */
+int daw_set_model_rho(daw_handle* h, const float* vp, const float* rho, int32_t n1, int32_t n2,
+                      int32_t npml, float hgrid, float dt, int32_t ofs);
+
 /* Datum receivers for the on-the-fly mode-2 resampling (rec_tab of the
  * mode-2 run, sub_redatum_DAW.f90:238; table as subacqui builds it). */
 int daw_set_datum(daw_handle* h, const int32_t* datum_tab, int32_t ndatum);

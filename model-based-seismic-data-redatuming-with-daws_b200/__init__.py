@@ -107,6 +107,7 @@ def _declare(L):
     L.daw_set_option.argtypes = [vp, i32, f64]
     L.daw_get_option.argtypes = [vp, i32, dp]
     L.daw_set_model.argtypes = [vp, fp, i32, i32, i32, f32, f32, i32]
+    L.daw_set_model_rho.argtypes = [vp, fp, fp, i32, i32, i32, f32, f32, i32]
     L.daw_set_datum.argtypes = [vp, ip, i32]
     L.daw_submodeling.argtypes = [vp, fp, i32, ip, i32, i32, ip, i32, fp, fp]
     L.daw_esource_data.argtypes = [vp, fp, i32, i32, ip, i32, fp]
@@ -227,11 +228,20 @@ class Handle:
         self._ck(lib().daw_get_option(self._h, OPT[key], C.byref(v)))
         return v.value
 
-    def set_model(self, vp, npml: int, h: float, dt: float, ofs: int):
+    def set_model(self, vp, npml: int, h: float, dt: float, ofs: int, rho=None):
+        """Velocity vp (n1, n2) and, optionally, density rho of the same shape
+        (None = rho 1, the reference's)."""
         vp = _f32(vp)
         n1, n2 = vp.shape
-        self._ck(lib().daw_set_model(self._h, _p(vp, C.c_float), n1, n2, npml, h, dt, ofs))
-        self.grid = dict(n1=n1, n2=n2, npml=npml, h=h, dt=dt, ofs=ofs)
+        if rho is None:
+            self._ck(lib().daw_set_model(self._h, _p(vp, C.c_float), n1, n2, npml, h, dt, ofs))
+        else:
+            rho = _f32(rho)
+            if rho.shape != vp.shape:
+                raise ValueError("rho must have the shape of vp")
+            self._ck(lib().daw_set_model_rho(self._h, _p(vp, C.c_float), _p(rho, C.c_float),
+                                             n1, n2, npml, h, dt, ofs))
+        self.grid = dict(n1=n1, n2=n2, npml=npml, h=h, dt=dt, ofs=ofs, rho=rho is not None)
 
     def set_datum(self, tab):
         tab = _i32(tab)

@@ -75,6 +75,12 @@ struct ModelDev {
   // prow[i1] = (d1a, d1a1, d1b, bw1), pcol[i2] = (d2a, d2a1, d2b, bw2).
   float4* prow = nullptr;
   float4* pcol = nullptr;
+  // With a density other than 1 (else null): the buoyancy-weighted update
+  // coefficients dtdx*bu1*damp1b1 and dtdx*bu2*damp2b1 and the buoyancy
+  // bu = 1/rho itself, on the extended grid ([n2e][ld]).
+  float* rbw1 = nullptr;
+  float* rbw2 = nullptr;
+  float* rbue = nullptr;
 };
 
 // A set of Hicks stations (sources or receivers) on the device.

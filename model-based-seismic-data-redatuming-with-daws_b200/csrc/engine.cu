@@ -254,6 +254,11 @@ void download(void* dst, const void* src, size_t bytes, cudaStream_t st) {
 
 void require_model(daw_handle* h) {
   if (!h->has_model) throw DawError{DAW_ERR_STATE, "no model: call daw_set_model first"};
+  // a density other than 1 runs on the plain and the split TMA kernels only
+  if (h->md.rbw1 && h->opt.fused && (h->opt.chunk != 0 || h->opt.step == 1))
+    throw DawError{DAW_ERR_ARG,
+                   "a model with density runs on the plain or the split TMA kernels "
+                   "(DAW_OPT_CHUNK = 0, DAW_OPT_STEP_KERNEL != 1)"};
 }
 
 void check_table(const daw_handle* h, const int32_t* tab, int n, bool extended, const char* what) {
@@ -496,7 +501,7 @@ void plain_forward(daw_handle* h, ShotCtx& c, float* sis, float* wf, float* red)
                      red, c.nt, it - 1, 1, 0, h->st);
     }
     plain_v_update(g, h->md, f, 2, +1, h->st);
-    if (c.type_src == 1) plain_inject(c.srcmap, c.vz, nullptr, g.dt, c.d_s + (it - 1), 0, +1, h->st);
+    if (c.type_src == 1) plain_inject(c.srcmap, c.vz, h->md.rbue, g.dt, c.d_s + (it - 1), 0, +1, h->st);
     plain_vz_free_surface(g, c.vz, h->st);
     h->tim.kernel_launches += 6;
   }
@@ -550,7 +555,7 @@ void plain_stage_b(daw_handle* h, ShotCtx& c, bool esource, float* out, int reve
                      red, c.nt, it - 1, 1, 0, h->st);
     }
     plain_v_update(g, h->md, f, 3, +1, h->st);
-    plain_vsrc(g, c.vx, c.vz, hist32(h, c, ic, 1), hist32(h, c, ic, 2), h->st);
+    plain_vsrc(g, h->md, c.vx, c.vz, hist32(h, c, ic, 1), hist32(h, c, ic, 2), h->st);
     plain_vz_free_surface(g, c.vz, h->st);
     h->tim.kernel_launches += 7;
   }
@@ -759,9 +764,9 @@ daw_handle::Tuned tune_run(daw_handle* h, Batch& b, int mode, FusedLaunch L, int
     return split_default;
   }
   char key[192];
-  std::snprintf(key, sizeof key, "m%d.f%d.g%dx%d.p%d.s%d.a%d.r%d.d%d.k%d.t%d.c%d", tmode, f,
-                h->g.n1, h->g.n2, h->g.npml, L.nshots, nact, L.max_rec, L.max_datum,
-                h->opt.step, h->opt.tile_cols, h->opt.ctas_per_sm);
+  std::snprintf(key, sizeof key, "m%d.f%d.g%dx%d.p%d.s%d.a%d.r%d.d%d.k%d.t%d.c%d.rho%d", tmode,
+                f, h->g.n1, h->g.n2, h->g.npml, L.nshots, nact, L.max_rec, L.max_datum,
+                h->opt.step, h->opt.tile_cols, h->opt.ctas_per_sm, h->md.rbw1 ? 1 : 0);
   auto found = h->tuned.find(key);
   if (found != h->tuned.end()) return found->second;
   const size_t n = b.shots.size();
@@ -823,7 +828,7 @@ daw_handle::Tuned tune_run(daw_handle* h, Batch& b, int mode, FusedLaunch L, int
         for (int vc = 1; vc <= occ_v; ++vc)
           if (!(timed && pc == occ_p && vc == occ_v)) consider({0, 32, pc, vc, kbest, 0.f});
   }
-  if (h->opt.step != 0)
+  if (h->opt.step != 0 && !h->md.rbw1)  // the step family has no density variant
     for (int tc : {16, 32}) {
       if (h->opt.tile_cols && h->opt.tile_cols != tc) continue;
       // a pinned CTA count above what fits is clamped to the occupancy
@@ -1972,9 +1977,11 @@ int daw_get_option(const daw_handle* h, int32_t key, double* value) {
   return DAW_OK;
 }
 
-int daw_set_model(daw_handle* h, const float* vp, int32_t n1, int32_t n2, int32_t npml,
-                  float hgrid, float dt, int32_t ofs) {
-  return guarded(h, [&] {
+namespace {
+
+// Model set-up of daw_set_model / daw_set_model_rho (submodeling2.f90:54-113).
+void set_model(daw_handle* h, const float* vp, const float* rho, int32_t n1, int32_t n2,
+               int32_t npml, float hgrid, float dt, int32_t ofs) {
     if (!vp || n1 < 4 || n2 < 4 || npml < 1 || !(hgrid > 0) || !(dt > 0))
       throw DawError{DAW_ERR_ARG, "daw_set_model: bad arguments"};
     sync(h);
@@ -1996,16 +2003,42 @@ int daw_set_model(daw_handle* h, const float* vp, int32_t n1, int32_t n2, int32_
     std::vector<float> bw1(g.n1e), bw2(g.n2e);
     for (int i = 0; i < g.n1e; ++i) bw1[i] = (g.dtdx * 1.0f) * d1b1[i];
     for (int i = 0; i < g.n2e; ++i) bw2[i] = (g.dtdx * 1.0f) * d2b1[i];
-    // kappa = rho vp^2 with rho = 1, formed in double (submodeling2.f90:1235)
-    // on the edge-replicated extended grid (submodext).
+    // kappa = rho vp^2, formed in double (submodeling2.f90:1235), on the
+    // edge-replicated extended grid (submodext); rho = 1 unless given.
     std::vector<float> kap(g.ext_elems(), 0.0f);
+    std::vector<float> bue(rho ? g.ext_elems() : 0, 1.0f);
     for (int j = 0; j < g.n2e; ++j) {
       const int sj = std::min(std::max(j - npml, 0), n2 - 1);
       for (int i = 0; i < g.n1e; ++i) {
         const int si = std::min(std::max(i - npml, 0), n1 - 1);
         const double v = (double)vp[si + (size_t)n1 * sj];
-        kap[i + (size_t)g.ld * j] = (float)(v * v);
+        const size_t k = i + (size_t)g.ld * j;
+        if (rho) {
+          const float r = rho[si + (size_t)n1 * sj];
+          kap[k] = (float)((double)r * (v * v));
+          bue[k] = r > 0.f ? 1.0f / r : 1e10f;  // substagger :1236-1240
+        } else {
+          kap[k] = (float)(v * v);
+        }
       }
+    }
+    // Buoyancy averaged onto the staggered grids (substagger :1248-1266):
+    // bu1 between rows i1 and i1+1, bu2 between columns i2 and i2+1, then
+    // the update coefficients dtdx*bu*damp*b1 (:107-108).  The last row of
+    // bu1 and the last column of bu2 are never read by the stencil (updates
+    // stop two points short of the edge); they keep bu itself.
+    std::vector<float> rbw1, rbw2;
+    if (rho) {
+      rbw1.assign(g.ext_elems(), 0.0f);
+      rbw2.assign(g.ext_elems(), 0.0f);
+      for (int j = 0; j < g.n2e; ++j)
+        for (int i = 0; i < g.n1e; ++i) {
+          const size_t k = i + (size_t)g.ld * j;
+          const float bu1 = i + 1 < g.n1e ? 0.5f * (bue[k + 1] + bue[k]) : bue[k];
+          const float bu2 = j + 1 < g.n2e ? 0.5f * (bue[k + g.ld] + bue[k]) : bue[k];
+          rbw1[k] = (g.dtdx * bu1) * d1b1[i];
+          rbw2[k] = (g.dtdx * bu2) * d2b1[j];
+        }
     }
     Pool& P = h->model_pool;
     ModelDev m;
@@ -2026,12 +2059,31 @@ int daw_set_model(daw_handle* h, const float* vp, int32_t n1, int32_t n2, int32_
     m.pcol = P.get_t<float4>("pcol", g.n2e);
     upload(m.prow, prow.data(), g.n1e * sizeof(float4), h->st);
     upload(m.pcol, pcol.data(), g.n2e * sizeof(float4), h->st);
+    if (rho) {
+      m.rbw1 = P.get_t<float>("rbw1", rbw1.size());
+      m.rbw2 = P.get_t<float>("rbw2", rbw2.size());
+      m.rbue = P.get_t<float>("rbue", bue.size());
+      upload(m.rbw1, rbw1.data(), rbw1.size() * 4, h->st);
+      upload(m.rbw2, rbw2.data(), rbw2.size() * 4, h->st);
+      upload(m.rbue, bue.data(), bue.size() * 4, h->st);
+    }
     sync(h);
     h->g = g;
     h->md = m;
     h->has_model = true;
     if (h->ndatum > 0) h->datum = make_stations(h, h->model_pool, "datum", h->datum_tab.data(), h->ndatum);
-  });
+}
+
+}  // namespace
+
+int daw_set_model(daw_handle* h, const float* vp, int32_t n1, int32_t n2, int32_t npml,
+                  float hgrid, float dt, int32_t ofs) {
+  return guarded(h, [&] { set_model(h, vp, nullptr, n1, n2, npml, hgrid, dt, ofs); });
+}
+
+int daw_set_model_rho(daw_handle* h, const float* vp, const float* rho, int32_t n1, int32_t n2,
+                      int32_t npml, float hgrid, float dt, int32_t ofs) {
+  return guarded(h, [&] { set_model(h, vp, rho, n1, n2, npml, hgrid, dt, ofs); });
 }
 
 int daw_set_datum(daw_handle* h, const int32_t* tab, int32_t n) {

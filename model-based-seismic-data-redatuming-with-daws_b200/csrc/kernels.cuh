@@ -102,8 +102,9 @@ void plain_store_interior(const Grid& g, float* dst, const float* src, bool accu
                           cudaStream_t st);
 void plain_psrc(const Grid& g, const ModelDev& m, float* px, const float* sp, bool esource,
                 cudaStream_t st);
-void plain_vsrc(const Grid& g, float* vx, float* vz, const float* svx, const float* svz,
-                cudaStream_t st);
+// v += -dt * s * bu (bu = 1 when the model has no density).
+void plain_vsrc(const Grid& g, const ModelDev& m, float* vx, float* vz, const float* svx,
+                const float* svz, cudaStream_t st);
 void plain_vz_free_surface(const Grid& g, float* vz, cudaStream_t st);
 
 // Hicks gather of `field` (leading dimension ld; `origin` is the address of

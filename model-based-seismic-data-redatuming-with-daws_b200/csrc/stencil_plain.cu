@@ -43,8 +43,10 @@ __global__ void __launch_bounds__(256) k_v_update(float* __restrict__ vx, float*
   const size_t k = i1 + (size_t)ld * i2;
   const float der2 = dplus(p[k - ld], p[k], p[k + ld], p[k + 2 * ld]);
   const float der1 = dplus(p[k - 1], p[k], p[k + 1], p[k + 2]);
-  const float ax = fmul(m.d2b[i2], vx[k]), bx = fmul(m.bw2[i2], der2);
-  const float az = fmul(m.d1b[i1], vz[k]), bz = fmul(m.bw1[i1], der1);
+  // coefficients: 1-D profiles for rho = 1, the 2-D buoyancy fields otherwise
+  const float bw2 = m.rbw2 ? m.rbw2[k] : m.bw2[i2], bw1 = m.rbw1 ? m.rbw1[k] : m.bw1[i1];
+  const float ax = fmul(m.d2b[i2], vx[k]), bx = fmul(bw2, der2);
+  const float az = fmul(m.d1b[i1], vz[k]), bz = fmul(bw1, der1);
   vx[k] = SIGN > 0 ? fadd(ax, bx) : fsub(ax, bx);
   vz[k] = SIGN > 0 ? fadd(az, bz) : fsub(az, bz);
 }
@@ -99,16 +101,18 @@ __global__ void k_psrc(float* __restrict__ px, const float* __restrict__ sp,
 
 // Stage-B velocity extended sources (:1175-1186), buoyancy 1.
 __global__ void k_vsrc(float* __restrict__ vx, float* __restrict__ vz,
-                       const float* __restrict__ svx, const float* __restrict__ svz, float dt,
-                       int n1, int n2, int npml, int ld) {
+                       const float* __restrict__ svx, const float* __restrict__ svz,
+                       const float* __restrict__ bue, float dt, int n1, int n2, int npml,
+                       int ld) {
   const int i1 = blockIdx.x * kBX + threadIdx.x;
   const int i2 = blockIdx.y * kBY + threadIdx.y;
   if (i1 >= n1 || i2 >= n2) return;
   const size_t k = (i1 + npml) + (size_t)ld * (i2 + npml);
   const size_t j = i1 + (size_t)n1 * i2;
   const float mdt = fmul(-1.0f, dt);
-  vx[k] = fadd(vx[k], fmul(fmul(mdt, svx[j]), 1.0f));
-  vz[k] = fadd(vz[k], fmul(fmul(mdt, svz[j]), 1.0f));
+  const float b = bue ? bue[k] : 1.0f;
+  vx[k] = fadd(vx[k], fmul(fmul(mdt, svx[j]), b));
+  vz[k] = fadd(vz[k], fmul(fmul(mdt, svz[j]), b));
 }
 
 // vz(npml,:) = vz(npml+1,:) (:260-264).
@@ -189,10 +193,10 @@ void plain_psrc(const Grid& g, const ModelDev& m, float* px, const float* sp, bo
                                                                g.npml, g.ld, lo, hi1, hi2);
 }
 
-void plain_vsrc(const Grid& g, float* vx, float* vz, const float* svx, const float* svz,
-                cudaStream_t st) {
-  k_vsrc<<<grid2(g.n1, g.n2), dim3(kBX, kBY), 0, st>>>(vx, vz, svx, svz, g.dt, g.n1, g.n2,
-                                                       g.npml, g.ld);
+void plain_vsrc(const Grid& g, const ModelDev& m, float* vx, float* vz, const float* svx,
+                const float* svz, cudaStream_t st) {
+  k_vsrc<<<grid2(g.n1, g.n2), dim3(kBX, kBY), 0, st>>>(vx, vz, svx, svz, m.rbue, g.dt, g.n1,
+                                                       g.n2, g.npml, g.ld);
 }
 
 void plain_vz_free_surface(const Grid& g, float* vz, cudaStream_t st) {

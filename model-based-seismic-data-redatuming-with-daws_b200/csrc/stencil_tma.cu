@@ -574,7 +574,11 @@ __global__ void __launch_bounds__(kThreadsT, 2)
 // ---------------------------------------------------------------------------
 // 3 CTAs per SM in the forward and stage-A modes (80 registers); the stage-B
 // modes keep 2 (their heavier body and tile count balance better at 2).
-template <int MODE, bool FP16>
+// RHO: a density other than 1 -- the update coefficients and the buoyancy
+// weight of the velocity sources come from the 2-D fields m.rbw1, m.rbw2 and
+// m.rbue (one float2 load per column and point pair) instead of the 1-D
+// sponge profiles and the constant 1.
+template <int MODE, bool FP16, bool RHO>
 __global__ void __launch_bounds__(kThreadsT,
                                   (MODE == FM_STAGE_B || MODE == FM_STAGE_B_ES) ? 2 : 3)
     k_tma_v(const Grid g, const ModelDev m, const FusedLaunch L, const int it, const int ntiles,
@@ -687,10 +691,10 @@ __global__ void __launch_bounds__(kThreadsT,
     if (live && !interior) {
       if (ok1) {
         d1b = ldg2(m.d1b + i1);
-        bw1 = ldg2(m.bw1 + i1);
+        if (!RHO) bw1 = ldg2(m.bw1 + i1);
       } else if (ok0) {
         d1b.x = __ldg(m.d1b + i1);
-        bw1.x = __ldg(m.bw1 + i1);
+        if (!RHO) bw1.x = __ldg(m.bw1 + i1);
       }
     }
     float d2b[CPT], bw2[CPT];
@@ -700,7 +704,7 @@ __global__ void __launch_bounds__(kThreadsT,
       const int c = cb + j;
       const bool cok = live && c < n2e;
       d2b[j] = cok && !interior ? __ldg(m.d2b + c) : 0.f;
-      bw2[j] = cok && !interior ? __ldg(m.bw2 + c) : 0.f;
+      bw2[j] = cok && !interior && !RHO ? __ldg(m.bw2 + c) : 0.f;
       clo[j] = (cok && do_inj) ? __ldg(sd.inj.col_lo + c) : 0x7fffffff;
       chi[j] = (cok && do_inj) ? __ldg(sd.inj.col_hi + c) : -1;
     }
@@ -739,13 +743,16 @@ __global__ void __launch_bounds__(kThreadsT,
           float2 vx_ = VX[cc * 32 + lane], vz_ = VZ[cc * 32 + lane];
           if (IN || (c >= 2 && c < hi2)) {
             const bool fwd = (MODE != FM_STAGE_A);
+            // k + 1 stays inside the padded column (i1 even, ld a multiple of 64)
+            const float2 rb2 = RHO ? ldg2(m.rbw2 + k) : make_float2(0.f, 0.f);
+            const float2 rb1 = RHO ? ldg2(m.rbw1 + k) : make_float2(0.f, 0.f);
             if (u0_) {
               const float der2 = dplus(a[j].x, pc.x, a[j + 2].x, a[j + 3].x);
               const float der1 = dplus(pm1, pc.x, pc.y, pp.x);
               const float ax = IN ? vx_.x : fmul(d2b[j], vx_.x);
-              const float bx = fmul(IN ? dtdx_v : bw2[j], der2);
+              const float bx = fmul(RHO ? rb2.x : IN ? dtdx_v : bw2[j], der2);
               const float az = IN ? vz_.x : fmul(d1b.x, vz_.x);
-              const float bz = fmul(IN ? dtdx_v : bw1.x, der1);
+              const float bz = fmul(RHO ? rb1.x : IN ? dtdx_v : bw1.x, der1);
               vx_.x = fwd ? fadd(ax, bx) : fsub(ax, bx);
               vz_.x = fwd ? fadd(az, bz) : fsub(az, bz);
             }
@@ -753,9 +760,9 @@ __global__ void __launch_bounds__(kThreadsT,
               const float der2 = dplus(a[j].y, pc.y, a[j + 2].y, a[j + 3].y);
               const float der1 = dplus(pc.x, pc.y, pp.x, pp.y);
               const float ax = IN ? vx_.y : fmul(d2b[j], vx_.y);
-              const float bx = fmul(IN ? dtdx_v : bw2[j], der2);
+              const float bx = fmul(RHO ? rb2.y : IN ? dtdx_v : bw2[j], der2);
               const float az = IN ? vz_.y : fmul(d1b.y, vz_.y);
-              const float bz = fmul(IN ? dtdx_v : bw1.y, der1);
+              const float bz = fmul(RHO ? rb1.y : IN ? dtdx_v : bw1.y, der1);
               vx_.y = fwd ? fadd(ax, bx) : fsub(ax, bx);
               vz_.y = fwd ? fadd(az, bz) : fsub(az, bz);
             }
@@ -763,22 +770,24 @@ __global__ void __launch_bounds__(kThreadsT,
           if (kB && cint && (r0_ || r1_)) {
             const float2 hx = hist_box_read<FP16>(st + kVStage, cc, lane);
             const float2 hz = hist_box_read<FP16>(st + kVStage + hist_box(FP16), cc, lane);
+            const float2 bu = RHO ? ldg2(m.rbue + k) : make_float2(1.0f, 1.0f);
             if (r0_) {
-              vx_.x = fadd(vx_.x, fmul(fmul(mdt, hx.x * sc_vx), 1.0f));
-              vz_.x = fadd(vz_.x, fmul(fmul(mdt, hz.x * sc_vz), 1.0f));
+              vx_.x = fadd(vx_.x, fmul(fmul(mdt, hx.x * sc_vx), bu.x));
+              vz_.x = fadd(vz_.x, fmul(fmul(mdt, hz.x * sc_vz), bu.x));
             }
             if (r1_) {
-              vx_.y = fadd(vx_.y, fmul(fmul(mdt, hx.y * sc_vx), 1.0f));
-              vz_.y = fadd(vz_.y, fmul(fmul(mdt, hz.y * sc_vz), 1.0f));
+              vx_.y = fadd(vx_.y, fmul(fmul(mdt, hx.y * sc_vx), bu.y));
+              vz_.y = fadd(vz_.y, fmul(fmul(mdt, hz.y * sc_vz), bu.y));
             }
           }
           if (i1 + 1 >= clo[j] && i1 <= chi[j]) {  // vz source (type_src = 1)
             const int base = __ldg(sd.inj.col_base + c) - clo[j];
+            const float2 bu = RHO ? ldg2(m.rbue + k) : make_float2(1.0f, 1.0f);
             if (i1 >= clo[j])
-              vz_.x = inject_at_global(sd.inj, vz_.x, base + i1, dt, 1.0f, sd.amp + (it - 1),
+              vz_.x = inject_at_global(sd.inj, vz_.x, base + i1, dt, bu.x, sd.amp + (it - 1),
                                        sd.amp_stride, +1);
             if (ok1_ && i1 + 1 <= chi[j])
-              vz_.y = inject_at_global(sd.inj, vz_.y, base + i1 + 1, dt, 1.0f, sd.amp + (it - 1),
+              vz_.y = inject_at_global(sd.inj, vz_.y, base + i1 + 1, dt, bu.y, sd.amp + (it - 1),
                                        sd.amp_stride, +1);
           }
           if (dst_x) vz_.x = vz_.y;
@@ -860,12 +869,21 @@ void launch_v(const Grid& g, const ModelDev& m, const FusedLaunch& L, int it, cu
   const int stations = (MODE == FM_STAGE_A) ? 0 : L.max_rec + L.max_datum;
   const int ngbps = (stations + 7) / 8;
   const int grid = std::max(1, std::min(std::max(ntiles, ngbps * L.nlive), L.persist_v));
-  if (L.hist_fp16)
-    launch_pdl(k_tma_v<MODE, true>, grid, kThreadsT, v_smem(MODE, true), st, L.pdl != 0, g, m, L,
-               it, ntiles, ngbps);
+  const bool fp16 = L.hist_fp16 != 0, rho = m.rbw1 != nullptr;
+  const size_t smem = v_smem(MODE, fp16);
+  const bool pdl = L.pdl != 0;
+  if (fp16 && !rho)
+    launch_pdl(k_tma_v<MODE, true, false>, grid, kThreadsT, smem, st, pdl, g, m, L, it, ntiles,
+               ngbps);
+  else if (!rho)
+    launch_pdl(k_tma_v<MODE, false, false>, grid, kThreadsT, smem, st, pdl, g, m, L, it, ntiles,
+               ngbps);
+  else if (fp16)
+    launch_pdl(k_tma_v<MODE, true, true>, grid, kThreadsT, smem, st, pdl, g, m, L, it, ntiles,
+               ngbps);
   else
-    launch_pdl(k_tma_v<MODE, false>, grid, kThreadsT, v_smem(MODE, false), st, L.pdl != 0, g, m,
-               L, it, ntiles, ngbps);
+    launch_pdl(k_tma_v<MODE, false, true>, grid, kThreadsT, smem, st, pdl, g, m, L, it, ntiles,
+               ngbps);
 }
 
 template <typename K>
@@ -879,7 +897,8 @@ int occupancy(K kernel, size_t smem) {
 template <int MODE, bool FP16>
 void prep_mode(int* pp, int* pv, int* pv_mode) {
   *pp = std::min(*pp, occupancy(k_tma_p<MODE, FP16>, p_smem(MODE, FP16)));
-  const int ov = occupancy(k_tma_v<MODE, FP16>, v_smem(MODE, FP16));
+  const int ov = std::min(occupancy(k_tma_v<MODE, FP16, false>, v_smem(MODE, FP16)),
+                          occupancy(k_tma_v<MODE, FP16, true>, v_smem(MODE, FP16)));
   *pv = std::min(*pv, ov);
   pv_mode[MODE * 2 + (FP16 ? 1 : 0)] = ov;
 }

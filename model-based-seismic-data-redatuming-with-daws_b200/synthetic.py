@@ -44,6 +44,13 @@ class Workload:
         return (((1.0 - 2.0 * a) * np.exp(-a)).astype(np.float32) / np.float32(self.h * self.h))
 
 
+def gardner(vp) -> np.ndarray:
+    """Gardner's density rho = 0.31 vp^0.25 (g/cm^3, vp in m/s) of a velocity
+    model, the density the benchmark configurations name (the reference
+    itself runs rho = 1)."""
+    return np.asfortranarray((0.31 * np.asarray(vp, np.float64) ** 0.25).astype(np.float32))
+
+
 def ricker_band(f0):
     # flow = 0.5 f0, fhig = 2.5 f0, llow = lhig = 0.5 f0
     return (0.5 * f0, 2.5 * f0, 0.5 * f0, 0.5 * f0)

@@ -199,6 +199,12 @@ std::vector<float> extend(const float* v, int n1, int n2, int npml) {
   return ve;
 }
 
+// Optional density of the next media (n1 x n2, column-major), set by
+// oracle_set_rho; empty = the reference's rho = 1.  Test infrastructure: one
+// setting for the whole process (not thread-safe).
+std::vector<float> g_rho;
+int g_rho_n1 = 0, g_rho_n2 = 0;
+
 template <typename T>
 Medium<T> make_medium(const float* vp, int n1, int n2, int npml, float h, float dt, int ofs) {
   Medium<T> m;
@@ -217,21 +223,38 @@ Medium<T> make_medium(const float* vp, int n1, int n2, int npml, float h, float 
   m.d2b.assign(d2b.begin(), d2b.end());
   // Density is identically 1 in the reference (src/submodeling2.f90:93), so
   // kappa = vp^2 (product formed in double, :1235), buoyancy = 1 and its
-  // staggered averages bu1 = bu2 = 1.
+  // staggered averages bu1 = bu2 = 1.  With a density set (oracle_set_rho),
+  // substagger (:1227-1270) on the edge-replicated grids: kappa = rho vp^2 in
+  // double, bu = 1/rho (1e10 where rho <= 0), bu1 = (bu(i1+1) + bu(i1))/2,
+  // bu2 = (bu(i2+1) + bu(i2))/2.  The last row of bu1 and the last column of
+  // bu2 (which the reference fills from a bu2 not yet computed, :1252) are
+  // never read: v_step stops two points short of the edge.  They keep bu.
   std::vector<float> ve = extend(vp, n1, n2, npml);
   const size_t np = (size_t)m.n1e * m.n2e;
+  const bool rho = !g_rho.empty() && g_rho_n1 == n1 && g_rho_n2 == n2;
+  std::vector<float> re = rho ? extend(g_rho.data(), n1, n2, npml) : std::vector<float>();
   m.kap.resize(np); m.kw1.resize(np); m.kw2.resize(np);
   m.bw1.resize(np); m.bw2.resize(np); m.bue.assign(np, (T)1);
+  std::vector<T> bu1(np, (T)1), bu2(np, (T)1);
+  if (rho) {
+    for (size_t k = 0; k < np; ++k) m.bue[k] = re[k] > 0.f ? (T)1 / (T)re[k] : (T)1e10;
+    for (int j = 0; j < m.n2e; ++j)
+      for (int i = 0; i < m.n1e; ++i) {
+        const size_t k = i + (size_t)m.n1e * j;
+        bu1[k] = i + 1 < m.n1e ? (T)0.5 * (m.bue[k + 1] + m.bue[k]) : m.bue[k];
+        bu2[k] = j + 1 < m.n2e ? (T)0.5 * (m.bue[k + m.n1e] + m.bue[k]) : m.bue[k];
+      }
+  }
   for (int j = 0; j < m.n2e; ++j)
     for (int i = 0; i < m.n1e; ++i) {
       size_t k = i + (size_t)m.n1e * j;
       double v = (double)ve[k];
-      T kap = (T)(v * v);
+      T kap = rho ? (T)((double)re[k] * (v * v)) : (T)(v * v);
       m.kap[k] = kap;
       m.kw2[k] = m.dtdx * kap * (T)d2a1[j];
       m.kw1[k] = m.dtdx * kap * (T)d1a1[i];
-      m.bw2[k] = m.dtdx * (T)1 * (T)d2b1[j];
-      m.bw1[k] = m.dtdx * (T)1 * (T)d1b1[i];
+      m.bw2[k] = m.dtdx * bu2[k] * (T)d2b1[j];
+      m.bw1[k] = m.dtdx * bu1[k] * (T)d1b1[i];
     }
   return m;
 }
@@ -867,6 +890,17 @@ int filmartin_weights(int nt, float dt, float flow, float fhig, float llow, floa
 // ---------------------------------------------------------------------------
 // C entry points (ctypes).  Suffix _f32: reference arithmetic; _f64: FP64.
 // ---------------------------------------------------------------------------
+
+extern "C" void oracle_set_rho(const float* rho, int n1, int n2) {
+  if (!rho || n1 <= 0 || n2 <= 0) {
+    g_rho.clear();
+    g_rho_n1 = g_rho_n2 = 0;
+    return;
+  }
+  g_rho.assign(rho, rho + (size_t)n1 * n2);
+  g_rho_n1 = n1;
+  g_rho_n2 = n2;
+}
 
 extern "C" {
 

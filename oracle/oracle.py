@@ -11,6 +11,7 @@ first index fastest; acquisition tables are (n, 5) int32 column-major.
 """
 from __future__ import annotations
 
+import contextlib
 import ctypes as C
 import os
 import subprocess
@@ -88,6 +89,8 @@ def _declare(L):
     L.oracle_baseline_sample.argtypes = [_f32p, i, i, i, f, i, i, f, _f32p, _i32p, _i32p, i,
                                          _f32p, f, i]
     L.oracle_baseline_sample.restype = d
+    L.oracle_set_rho.argtypes = [_opt(_f32p), i, i]
+    L.oracle_set_rho.restype = None
 
 
 def _dt(prec):
@@ -137,6 +140,26 @@ def sponges(npml: int, n: int):
     a, a1, b, b1 = (np.zeros(n + 2 * npml, np.float32) for _ in range(4))
     lib().oracle_sponges(npml, n, a, a1, b, b1)
     return a, a1, b, b1
+
+
+@contextlib.contextmanager
+def density(rho):
+    """Runs the enclosed oracle calls with density rho (then back to 1)."""
+    set_rho(rho)
+    try:
+        yield
+    finally:
+        set_rho(None)
+
+
+def set_rho(rho=None):
+    """Density (n1, n2) of the media that later calls build (None = 1, the
+    reference's); one process-wide setting (test infrastructure)."""
+    if rho is None:
+        lib().oracle_set_rho(None, 0, 0)
+    else:
+        r = _f(rho, np.float32)
+        lib().oracle_set_rho(r, r.shape[0], r.shape[1])
 
 
 # -- simulations -------------------------------------------------------------

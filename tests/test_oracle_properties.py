@@ -103,3 +103,71 @@ def test_homogeneous_green_function(O):
         scale = np.dot(num, ana) / np.dot(ana, ana)
         assert rel_l2(num, scale * ana) < 0.1
         assert 0.9 < scale < 1.1, scale
+
+
+def _sources(O, vp, npml, h, nt):
+    ir = O.acqui_table([[15.0, x] for x in np.linspace(0, 450, 7)], h, npml, 1)
+    is5 = O.acqui_table([[25.0, 230.0]], h, npml, 1)[0]
+    s = np.sin(np.arange(nt) * 0.2).astype(np.float32) * np.exp(-np.arange(nt) * 0.02).astype(np.float32)
+    return ir, is5, s
+
+
+def test_density_one_is_the_reference(O):
+    """A density of 1 given explicitly runs the reference's rho = 1 arithmetic
+    bit for bit (substagger, submodeling2.f90:1227-1270)."""
+    vp, npml, h, dt, nt = _case()
+    ir, is5, s = _sources(O, vp, npml, h, nt)
+    res = np.asfortranarray(np.random.default_rng(4).standard_normal((nt, 7)).astype(np.float32))
+    a, _ = O.submodeling(vp, npml, h, 1, nt, dt, s, is5, ir)
+    v, _ = O.submodeling(vp, npml, h, 1, nt, dt, s, is5, ir, type_src=1)
+    g = O.esource_data(vp, npml, h, 1, nt, dt, res, ir)
+    e, _, _ = O.esource(vp, npml, h, 1, nt, dt, res, ir, want_wavefield=False)
+    with O.density(np.ones_like(vp)):
+        assert np.array_equal(O.submodeling(vp, npml, h, 1, nt, dt, s, is5, ir)[0], a)
+        assert np.array_equal(O.submodeling(vp, npml, h, 1, nt, dt, s, is5, ir, type_src=1)[0], v)
+        assert np.array_equal(O.esource_data(vp, npml, h, 1, nt, dt, res, ir), g)
+        assert np.array_equal(O.esource(vp, npml, h, 1, nt, dt, res, ir, want_wavefield=False)[0], e)
+
+
+def test_density_power_of_two_scaling(O):
+    """rho = 2 doubles kappa and halves the buoyancy: the pressure of a
+    pressure source doubles exactly, and that of a velocity source (weighted
+    by the buoyancy, :252) is unchanged bit for bit (power-of-two scalings
+    commute with rounding)."""
+    vp, npml, h, dt, nt = _case()
+    ir, is5, s = _sources(O, vp, npml, h, nt)
+    a, _ = O.submodeling(vp, npml, h, 1, nt, dt, s, is5, ir)
+    v, _ = O.submodeling(vp, npml, h, 1, nt, dt, s, is5, ir, type_src=1)
+    with O.density(np.full_like(vp, 2.0)):
+        a2, _ = O.submodeling(vp, npml, h, 1, nt, dt, s, is5, ir)
+        v2, _ = O.submodeling(vp, npml, h, 1, nt, dt, s, is5, ir, type_src=1)
+    assert np.array_equal(a2, 2 * a)
+    assert np.array_equal(v2, v)
+
+
+@pytest.mark.parametrize("rho2", [2.0, 0.5])
+def test_density_contrast_reflection(O, rho2):
+    """A density step at constant velocity reflects with R = (rho2 - rho1) /
+    (rho2 + rho1) at every angle (equal velocities: no refraction).  The
+    reflected wave (the difference from the rho = 1 run) is compared with
+    R times the direct wave of the rho = 1 run at the image distance."""
+    n1 = n2 = 121
+    npml, h, dt, nt, c = 30, 10.0, 0.001, 500, 2000.0
+    vp = np.full((n1, n2), c, np.float32, order="F")
+    rho = np.ones((n1, n2), np.float32, order="F")
+    rho[61:, :] = rho2  # interface between rows 60 and 61 (z = 600-610 m)
+    f0 = 12.0
+    t = np.arange(nt) * dt - 1.0 / f0
+    s = (((1 - 2 * (np.pi * f0 * t) ** 2) * np.exp(-(np.pi * f0 * t) ** 2)) / h ** 2).astype(np.float32)
+    src = O.acqui_table([[300.0, 600.0]], h, npml, 0)[0]
+    ir = O.acqui_table([[300.0, 650.0], [905.0, 650.0]], h, npml, 0)
+    hom, _ = O.submodeling(vp, npml, h, 0, nt, dt, s, src, ir, prec="f64")
+    with O.density(rho):
+        het, _ = O.submodeling(vp, npml, h, 0, nt, dt, s, src, ir, prec="f64")
+    refl = het[:, 0] - hom[:, 0]
+    image = hom[:, 1]  # 605 m below the source: the image source's distance
+    R = np.sign(np.dot(refl, image)) * np.max(np.abs(refl)) / np.max(np.abs(image))
+    expect = (rho2 - 1.0) / (rho2 + 1.0)
+    assert abs(R - expect) < 0.03, (R, expect)
+    # arrival time within a few samples of the image wave's
+    assert abs(int(np.argmax(np.abs(refl))) - int(np.argmax(np.abs(image)))) <= 8
