@@ -105,7 +105,16 @@ def workload_text(w, args):
     return txt
 
 
-def shot_dicts(pkg, h, w, ids, model_dobs=True):
+def densities(w, args):
+    """(rho of the true model, rho of the background model): None for the
+    reference's rho = 1, or Gardner's relation of each velocity model."""
+    if getattr(args, "density", "1") != "gardner":
+        return None, None
+    from daw_b200 import synthetic
+    return synthetic.gardner(w.vtrue), synthetic.gardner(w.c0)
+
+
+def shot_dicts(pkg, h, w, ids, model_dobs=True, rho=(None, None)):
     """The shots `ids` of the workload; observed data modelled in the true
     model (mode 0, batched) on the GPU.  Reduced profiling variants use dobs =
     0: their records are too short for a reflection to separate the models,
@@ -118,14 +127,14 @@ def shot_dicts(pkg, h, w, ids, model_dobs=True):
         shots.append(dict(s=w.wavelet(nt), nt=nt, src=src, rec=rec, mu=w.mu, maxiter=w.maxiter,
                           rtol=0.0, band=w.band, shot=i + 1))
     if model_dobs:
-        h.set_model(w.vtrue, w.npml, w.h, w.dt, w.ofs)
+        h.set_model(w.vtrue, w.npml, w.h, w.dt, w.ofs, rho=rho[0])
         data = h.submodeling_shots(shots)
         for sh, d in zip(shots, data):
             sh["dobs"] = d
     else:
         for sh in shots:
             sh["dobs"] = np.zeros((sh["nt"], sh["rec"].shape[0]), np.float32, order="F")
-    h.set_model(w.c0, w.npml, w.h, w.dt, w.ofs)
+    h.set_model(w.c0, w.npml, w.h, w.dt, w.ofs, rho=rho[1])
     h.set_datum(pkg.subacqui(w.datum_pos, w.h, w.npml, w.ofs))
     return shots
 
@@ -307,25 +316,32 @@ def op_steps_per_application(nt, window):
     return nt + (nt - last) + (2 * nwin - 1) + nt
 
 
-def roofline(tim, w, fp16=True):
+def roofline(tim, w, fp16=True, rho=False):
     """The step kernels of the G G^T stages (stage A and stage B, one launch
     per time step): algorithmic bytes per shot step = 36 B per extended point
     (px, pz, vx, vz read and written, kappa read) + 3 history fields per
     interior point (written in stage A, read in stage B: 2 B each in FP16),
-    over the device time of those time loops."""
+    over the device time of those time loops.  With a density, the two
+    buoyancy coefficient fields add 8 B per extended point, and the buoyancy
+    weight of stage B's velocity sources 4 B per interior point of a stage-B
+    step."""
     peaks = json.load(open(PEAKS)) if os.path.exists(PEAKS) else {}
     peak = peaks.get("hbm_gbs", 6650.0)
     ne = (w.n1 + 2 * w.npml) * (w.n2 + 2 * w.npml)
     ni = w.n1 * w.n2
-    per_shot_step = 36.0 * ne + 3 * (2 if fp16 else 4) * ni
+    per_shot_step = 36.0 * ne + 3 * (2 if fp16 else 4) * ni + (8.0 * ne if rho else 0.0)
     shot_steps = tim["shot_steps_a"] + tim["shot_steps_b"]
+    if rho:  # averaged over the stage-A and stage-B shot steps
+        per_shot_step += 4.0 * ni * tim["shot_steps_b"] / max(shot_steps, 1)
     ms = tim["sim_a_ms"] + tim["sim_b_ms"]
     launches = tim["steps_a"] + tim["steps_b"]
     achieved = per_shot_step * shot_steps / (ms * 1e-3) / 1e9
     avg_ms = ms / max(launches, 1)
     bytes_per_launch = per_shot_step * shot_steps / max(launches, 1)
     traffic, note = None, None
-    if os.path.exists(TRAFFIC):
+    if rho:
+        note = "the committed ncu traffic capture ran rho = 1; none for this density"
+    elif os.path.exists(TRAFFIC):
         t = json.load(open(TRAFFIC))
         traffic = t["bytes_per_shot_step"] * shot_steps / max(launches, 1)
         note = t["note"]
@@ -346,7 +362,7 @@ def reference_runs(pkg, local, shots, base_out):
     for name, preset, opt in (("plain_fp32", "plain", {}),
                               ("fused_fp32", "mixed", {"history": 0, "scalars": 0})):
         with pkg.Handle(local, preset=preset, **opt) as h:
-            h.set_model(*base_out["model"])
+            h.set_model(*base_out["model"], rho=base_out["rho"])
             h.set_datum(base_out["datum"])
             ms, outs, launches, i = 0.0, [], 0, 0
             try:
@@ -424,7 +440,7 @@ def run_ours(args):
     cap = args.batch if args.config == 2 else 8
     h = pkg.Handle(local, preset="mixed", checkpoint=args.checkpoint,
                    step={"split": 0, "step": 1, "auto": 2}[args.kernel], tile_cols=args.tile_cols,
-                   ctas_per_sm=args.ctas_per_sm, pdl=0 if args.no_pdl else 1)
+                   ctas_per_sm=args.ctas_per_sm, pdl=1 if args.pdl else 0)
     if args.config in (2, 5):
         per_step = args.batch
         need = per_step
@@ -433,7 +449,8 @@ def run_ours(args):
     ids = [mine[i % len(mine)] for i in range(need)]
     # reduced records end before a reflection separates the true and
     # background models: observed data zero (residual = -datar) there
-    shots = shot_dicts(pkg, h, w, ids, model_dobs=not variant)
+    rho = densities(w, args)
+    shots = shot_dicts(pkg, h, w, ids, model_dobs=not variant, rho=rho)
     cfg5 = cfg5_checks(pkg, h, w, shots, args) if args.config == 5 else None
     # config 4: batches of similar record lengths (the shots sorted by nt,
     # each batch as many as HBM admits, as daw_shots forms them), run in a
@@ -490,7 +507,7 @@ def run_ours(args):
     total_ms = ranks.max_over_ranks(dist, sum(dev_ms))
     shots_done = ranks.sum_over_ranks(dist, sum(step_shots))
     value = shots_done * 3600.0 / (total_ms * 1e-3)
-    roof = roofline(tim, w)
+    roof = roofline(tim, w, rho=rho[1] is not None)
     upd_per_s = tim["point_updates"] / (sum(dev_ms) * 1e-3) * world
     # mixed outputs of the first timed batch (accuracy against FP32 histories)
     mixed_first = None
@@ -527,7 +544,8 @@ def run_ours(args):
     del h
     plain = fused = acc = None
     if rank == 0 and not args.no_plain:
-        refs = reference_runs(pkg, local, first_batch, {"model": model, "datum": datum})
+        refs = reference_runs(pkg, local, first_batch,
+                              {"model": model, "datum": datum, "rho": rho[1]})
         out32 = refs["fused_fp32"].pop("outs")
         outp = refs["plain_fp32"].pop("outs")
         per_shot_value = value / world
@@ -596,14 +614,17 @@ def run_ours(args):
                        "batching": ("shots sorted by record length, as many per batch as HBM "
                                     "admits, batches in seeded shuffled order"
                                     if args.config == 4 else f"{args.batch} shots per batch"),
-                       "density": "1 (the reference's rho = 1, src/submodeling2.f90:93)",
+                       "density": ("Gardner, rho = 0.31 vp^0.25 of each velocity model (the "
+                                   "configuration's; the reference runs rho = 1)"
+                                   if args.density == "gardner" else
+                                   "1 (the reference's rho = 1, src/submodeling2.f90:93)"),
                        "kernel": {"auto": "TMA time-step kernels, family and launch shape "
                                           "autotuned per mode",
                                   "split": "TMA pressure and velocity kernels, shots per launch "
                                            "and CTAs per SM autotuned per mode",
                                   "step": "one TMA kernel per time step (p recomputed on the "
                                           "v halo)"}[args.kernel]
-                                 + ("" if args.no_pdl else ", programmatic dependent launch"),
+                                 + (", programmatic dependent launch" if args.pdl else ""),
                        "autotuned": tc,
                        "parallelism": f"shots x{world} (para_range, no collective)",
                        "stage_a_history": (f"windows of {args.checkpoint} steps (checkpointed)"
@@ -678,12 +699,15 @@ def main():
     # A/B: the one-kernel-per-step path (default) or the split p / v kernels
     # the TMA kernel family: autotuned (default), split p / v kernels, or one per step
     ap.add_argument("--kernel", default="split", choices=["split", "step", "auto"])
-    ap.add_argument("--no-pdl", action="store_true", help="plain stream order between steps")
+    ap.add_argument("--pdl", action="store_true",
+                    help="programmatic dependent launch between steps (default: stream order)")
     # pin the step kernel's tile width / CTAs per SM (0 = autotuned)
     ap.add_argument("--tile-cols", type=int, default=0, choices=[0, 16, 32])
     ap.add_argument("--ctas-per-sm", type=int, default=0)
     # stage-A history in windows of K steps (checkpointed; one shot per launch)
     ap.add_argument("--checkpoint", type=int, default=0)
+    ap.add_argument("--density", default="1", choices=["1", "gardner"],
+                    help="rho = 1 (the reference's) or Gardner's rho = 0.31 vp^0.25")
     args = ap.parse_args()
     if args.batch is None:
         args.batch = 1 if args.config == 5 else 2
