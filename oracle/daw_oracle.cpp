@@ -199,11 +199,11 @@ std::vector<float> extend(const float* v, int n1, int n2, int npml) {
   return ve;
 }
 
-// Optional density of the next media (n1 x n2, column-major), set by
-// oracle_set_rho; empty = the reference's rho = 1.  Test infrastructure: one
-// setting for the whole process (not thread-safe).
-std::vector<float> g_rho;
-int g_rho_n1 = 0, g_rho_n2 = 0;
+// Optional density of the media that later calls of the same thread build
+// (n1 x n2, column-major), set by oracle_set_rho; empty = the reference's
+// rho = 1.  Per thread, so concurrent oracle calls do not see each other's.
+thread_local std::vector<float> g_rho;
+thread_local int g_rho_n1 = 0, g_rho_n2 = 0;
 
 template <typename T>
 Medium<T> make_medium(const float* vp, int n1, int n2, int npml, float h, float dt, int ofs) {

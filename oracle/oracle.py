@@ -144,7 +144,8 @@ def sponges(npml: int, n: int):
 
 @contextlib.contextmanager
 def density(rho):
-    """Runs the enclosed oracle calls with density rho (then back to 1)."""
+    """Runs the enclosed oracle calls of this thread with density rho (then
+    back to 1)."""
     set_rho(rho)
     try:
         yield
@@ -153,8 +154,8 @@ def density(rho):
 
 
 def set_rho(rho=None):
-    """Density (n1, n2) of the media that later calls build (None = 1, the
-    reference's); one process-wide setting (test infrastructure)."""
+    """Density (n1, n2) of the media that later calls of this thread build
+    (None = 1, the reference's)."""
     if rho is None:
         lib().oracle_set_rho(None, 0, 0)
     else:

@@ -147,11 +147,65 @@ def test_kernels_without_density_refuse_it(pkg, case, opt):
             h.submodeling(case["s"], case["src"], case["rec"])
 
 
+def _with_density(O, rho, fn, *args, **kw):
+    with O.density(rho):
+        return fn(*args, **kw)
+
+
+NT2 = 200
+
+
+def test_751x2301_forward_and_ggt_bitexact(pkg, O):
+    """The benchmark grid (751x2301, h = 4 m, npml 40, 576 receivers) with
+    Gardner density, nt 200: forward modelling (pressure and velocity
+    sources) and G G^T of the plain port and the split TMA kernels (FP32
+    histories) against the FP32 oracle, bit for bit.  The oracle runs in
+    worker threads while the GPU runs."""
+    from concurrent.futures import ThreadPoolExecutor
+    from daw_b200 import synthetic
+    w = synthetic.config2(nshot=1, nt=NT2)
+    rho = synthetic.gardner(w.c0)
+    src = pkg.subacqui(w.src_pos, w.h, w.npml, w.ofs)[0]
+    rec = pkg.subacqui(w.rec_pos[0], w.h, w.npml, w.ofs)
+    s = w.wavelet(NT2 + 140)[140:].copy()  # Ricker peak at step 60
+    args = (w.c0, w.npml, w.h, w.ofs, NT2, w.dt)
+    with ThreadPoolExecutor(3) as pool:
+        fut = {t: pool.submit(_with_density, O, rho, O.submodeling, *args, s, src, rec,
+                              type_src=t) for t in (0, 1)}
+        dobs = fut[0].result()[0]
+        res = np.asfortranarray(dobs[::-1])
+        fut["ggt"] = pool.submit(_with_density, O, rho, O.esource_data, *args, res, rec)
+        got = {}
+        for preset, opt in (("plain", {}), ("mixed", {"history": 0})):
+            with pkg.Handle(0, preset=preset, **opt) as h:
+                h.set_model(w.c0, w.npml, w.h, w.dt, w.ofs, rho=rho)
+                got[preset] = ([h.submodeling(s, src, rec, type_src=t)[0] for t in (0, 1)],
+                               h.submodeling_adjoint_esource_data(res, rec))
+        ref = ([fut[0].result()[0], fut[1].result()[0]], fut["ggt"].result())
+    assert np.abs(ref[0][0]).max() > 0
+    for preset, (fw, g) in got.items():
+        for t in (0, 1):
+            assert np.array_equal(fw[t], ref[0][t]), (preset, t)
+        assert np.array_equal(g, ref[1]), preset
+
+
+def _equal_above_precursor(a, b):
+    """a == b bit for bit wherever |b| > 1e-6 max|b|; below, |a - b| <=
+    1e-9 max|b|.  A power-of-two scaling commutes with rounding except in the
+    FP32 subnormal range, reached by the stencil's exponentially small
+    precursor ahead of the wavefront; its 1-ulp differences grow with the
+    precursor but stay many decades below the signal."""
+    peak = np.abs(b).max()
+    big = np.abs(b) > 1e-6 * peak
+    assert np.array_equal(a[big], b[big])
+    assert np.abs(a - b).max() <= 1e-9 * peak
+
+
 def test_power_of_two_density_on_751x2301(pkg):
     """Size-independent identity on the benchmark grid (751x2301, h = 4 m,
-    576 receivers, FP16-history mixed preset): rho = 2 doubles kappa and
-    halves the buoyancy, so a pressure source's data double exactly and a
-    velocity source's are unchanged bit for bit."""
+    576 receivers, FP16-history mixed preset, nt 300): rho = 2 doubles kappa
+    and halves the buoyancy, so a pressure source's data double and a
+    velocity source's are unchanged (exactly, above the precursor)."""
     from daw_b200 import synthetic
     w = synthetic.config2(nshot=1, nt=300)
     src = pkg.subacqui(w.src_pos, w.h, w.npml, w.ofs)[0]
@@ -164,5 +218,5 @@ def test_power_of_two_density_on_751x2301(pkg):
                         rho=None if r is None else np.full_like(w.c0, r))
             out[r] = [h.submodeling(s, src, rec, type_src=t)[0] for t in (0, 1)]
     assert np.abs(out[None][0]).max() > 0
-    assert np.array_equal(out[2.0][0], 2 * out[None][0])
-    assert np.array_equal(out[2.0][1], out[None][1])
+    _equal_above_precursor(out[2.0][0], 2 * out[None][0])
+    _equal_above_precursor(out[2.0][1], out[None][1])
