@@ -220,3 +220,34 @@ def test_power_of_two_density_on_751x2301(pkg):
     assert np.abs(out[None][0]).max() > 0
     _equal_above_precursor(out[2.0][0], 2 * out[None][0])
     _equal_above_precursor(out[2.0][1], out[None][1])
+
+
+def test_batched_windowed_shots_with_density(pkg, O, case):
+    """Three uneven shots with density in one batch equal the same shots run
+    one at a time, and stage-A history windows change no bit."""
+    w = case["w"]
+    shots = []
+    for k, (nt, lo, hi, x) in enumerate([(400, 0, 24, 300.0), (330, 4, 17, 520.0),
+                                         (371, 10, 24, 700.0)]):
+        src = pkg.subacqui([[15.0, x]], w.h, w.npml, w.ofs)[0]
+        rec = case["rec"][lo:hi]
+        s = w.wavelet(nt)
+        with O.density(synthetic_rho_true(case)):
+            dobs, _ = O.submodeling(w.vtrue, w.npml, w.h, w.ofs, nt, w.dt, s, src, rec)
+        shots.append(dict(s=s, nt=nt, src=src, rec=rec, dobs=dobs, mu=w.mu, maxiter=3,
+                          rtol=0.0, band=w.band, shot=k + 1))
+    with handle(pkg, case, "mixed") as h:
+        h.set_datum(case["ird"])
+        batched = h.shots(shots)
+        single = [h.shots([sh])[0] for sh in shots]
+        h.set_options(checkpoint=37)
+        windowed = h.shots(shots)
+    for b, s1, s2 in zip(batched, single, windowed):
+        for key in ("deltade", "dataesc", "redatumed"):
+            assert np.array_equal(b[key], s1[key]), key
+            assert np.array_equal(b[key], s2[key]), key
+
+
+def synthetic_rho_true(case):
+    from daw_b200 import synthetic
+    return synthetic.gardner(case["w"].vtrue)
