@@ -1,6 +1,8 @@
-"""Host-side arithmetic of bench.py's checkpointed variant (CPU only): the
-number of time steps one G G^T application runs, with and without stage-A
-history windows, which is the divisor of the roofline's average step time."""
+"""Host-side arithmetic of bench.py (CPU only): the number of time steps one
+G G^T application runs, with and without stage-A history windows (the
+divisor of the roofline's average step time), the roofline's algorithmic
+bytes with and without a density, and the Gardner density of its density
+switch."""
 import importlib.util
 import os
 import subprocess
@@ -40,3 +42,38 @@ def test_checkpoint_needs_one_shot_per_launch():
                         "--batch", "2"], capture_output=True, text=True, cwd=ROOT, timeout=120)
     assert r.returncode == 2
     assert "--batch 1" in r.stderr
+
+
+def test_roofline_bytes_with_density():
+    """Algorithmic bytes per shot step: 36 B per extended point + 6 B of FP16
+    history per interior point; a density adds the two buoyancy coefficient
+    fields (8 B per extended point) and stage B's buoyancy weight (4 B per
+    interior point of a stage-B step, here half the shot steps)."""
+    from types import SimpleNamespace
+    b = _bench()
+    w = SimpleNamespace(n1=751, n2=2301, npml=40)
+    tim = dict(shot_steps_a=100, shot_steps_b=100, sim_a_ms=2.0, sim_b_ms=2.0, steps_a=50,
+               steps_b=50)
+    ne, ni = 831 * 2381, 751 * 2301
+    r1 = b.roofline(tim, w)
+    r2 = b.roofline(tim, w, rho=True)
+    assert r1["bytes_per_shot_step"] == 36 * ne + 6 * ni
+    assert r2["bytes_per_shot_step"] == 36 * ne + 6 * ni + 8 * ne + 2 * ni
+    assert r2["traffic"] is None  # the committed traffic capture ran density 1
+    assert abs(r2["achieved"] / r1["achieved"] - r2["bytes_per_shot_step"] / r1["bytes_per_shot_step"]) < 1e-12
+
+
+def test_gardner_density():
+    import numpy as np
+    b = _bench()
+    b.entry.load_package()
+    from daw_b200 import synthetic
+    rho = synthetic.gardner(np.array([[1500.0, 2000.0], [4000.0, 5500.0]]))
+    assert rho.dtype == np.float32 and rho.flags.f_contiguous
+    assert np.allclose(rho, 0.31 * np.array([[1500.0, 2000.0], [4000.0, 5500.0]]) ** 0.25, rtol=1e-6)
+    from types import SimpleNamespace
+    w = SimpleNamespace(vtrue=np.full((3, 4), 2000.0), c0=np.full((3, 4), 1500.0))
+    rt, r0 = b.densities(w, SimpleNamespace(density="gardner"))
+    assert rt.shape == (3, 4) and abs(float(rt[0, 0]) - 0.31 * 2000.0 ** 0.25) < 1e-5
+    assert abs(float(r0[0, 0]) - 0.31 * 1500.0 ** 0.25) < 1e-5
+    assert b.densities(w, SimpleNamespace(density="1")) == (None, None)
