@@ -57,3 +57,44 @@ def test_driver_executable_exists(pkg):
     import os
     exe = os.path.join(os.path.dirname(pkg.LIB_PATH), "main_redatum_daw")
     assert os.access(exe, os.X_OK)
+
+
+C_CLIENT = r"""
+#include <math.h>
+#include <stdio.h>
+#include "daw_b200.h"
+
+int main(void) {
+  float tile[21 * 21];
+  double sum = 0.0;
+  int32_t loc[5];
+  daw_handle* h = NULL;
+  int rc;
+  daw_hicks_tile(51, 51, 0, tile);           /* on-node monopole: sums to 1 */
+  for (int i = 0; i < 21 * 21; ++i) sum += tile[i];
+  daw_hicks_locate(40.0f, 100.0f, 20.0f, 1, loc);
+  rc = daw_create(&h, 0);
+  if (rc == DAW_OK) daw_destroy(h);
+  printf("%.6f %d %d %d %d %d %d\n", sum, loc[0], loc[1], loc[2], loc[3], loc[4], rc);
+  return 0;
+}
+"""
+
+
+def test_header_is_plain_c(pkg, tmp_path):
+    """include/daw_b200.h compiles as C99 and a C client links the library:
+    the boundary a Fortran (ISO_C_BINDING) or any C-FFI caller binds."""
+    import os
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    src = tmp_path / "client.c"
+    src.write_text(C_CLIENT)
+    exe = tmp_path / "client"
+    libdir = os.path.dirname(pkg.LIB_PATH)
+    subprocess.run(["gcc", "-std=c99", "-Wall", "-Werror", "-pedantic",
+                    "-I", os.path.join(root, "include"), str(src), "-o", str(exe),
+                    "-L", libdir, "-ldaw_b200", "-Wl,-rpath," + libdir, "-lm"],
+                   check=True, capture_output=True, text=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split()
+    assert abs(float(out[0]) - 1.0) < 1e-5
+    assert [int(v) for v in out[1:6]] == [3, 6, 51, 51, 8]  # subsourcekws on a grid node
+    assert int(out[6]) in (0, -8)  # a handle on a GPU box, DAW_ERR_NODEV without one
