@@ -727,9 +727,11 @@ void stop_clock(daw_handle* h, SimClock& clk, Batch& b, int mode, const Window* 
 }
 
 // Autotuner of the TMA time-step kernels, per (mode, history precision,
-// grid, batch).  Candidates are timed over the run's first two steps (so the
-// one-kernel-per-step family's work deferred to the next launch is counted),
-// median of 3 after a warm-up, and compared by device time per shot step:
+// grid, batch).  Candidates are timed over the run's first six steps (at
+// least two, so the one-kernel-per-step family's work deferred to the next
+// launch is counted; six, so a 20-40 us step is timed well above the event
+// resolution), median of 3 after a warm-up, and compared by device time per
+// shot step:
 //   - separate pressure and velocity kernels (64 x 32 tiles): the shots per
 //     launch -- an HBM-admitted batch can run its time loops in groups of k
 //     shots, and the fastest k is often below the batch because the groups'
@@ -782,7 +784,7 @@ daw_handle::Tuned tune_run(daw_handle* h, Batch& b, int mode, FusedLaunch L, int
       T.tile_cols = cd.tile_cols;
       T.smaps = b.d_smaps + (cd.tile_cols == 32 ? n : 0);
     }
-    const int nst = std::min(first + 1, last_step) - first + 1;
+    const int nst = std::min(first + 5, last_step) - first + 1;
     float ms[3];
     for (int r = 0; r < 4; ++r) {
       if (cd.family == 1) CK(cudaMemsetAsync(h->d_qctr, 0, sizeof(unsigned), h->st));
