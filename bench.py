@@ -73,7 +73,19 @@ def rel(a, b):
 # ---------------------------------------------------------------------------
 # workloads
 # ---------------------------------------------------------------------------
-def make_workload(config=4, nt=None):
+def make_workload(config=4, nt=None, maxiter=None):
+    """The workload of --config (4: the 256-shot uneven set; 2: the uniform
+    50-shot set; 5: the 2001x8001 grid, reduced to nt 1000 and 2 MINRES
+    iterations unless given)."""
+    w = _workload(config, nt)
+    if maxiter is not None:
+        w.maxiter = maxiter
+    elif config == 5:
+        w.maxiter = 2
+    return w
+
+
+def _workload(config, nt):
     entry.load_package()
     from daw_b200 import synthetic
     if config == 4:
@@ -112,6 +124,22 @@ def densities(w, args):
         return None, None
     from daw_b200 import synthetic
     return synthetic.gardner(w.vtrue), synthetic.gardner(w.c0)
+
+
+def bench_config(w, args, world):
+    """The workload the line was measured on; both arms print the same."""
+    return {"workload": workload_text(w, args),
+            "batching": ("shots sorted by record length, as many per batch as HBM admits, "
+                         "batches in seeded shuffled order"
+                         if args.config == 4 else f"{args.batch} shots per batch"),
+            "density": ("Gardner, rho = 0.31 vp^0.25 of each velocity model (the "
+                        "configuration's; the reference runs rho = 1)"
+                        if args.density == "gardner" else
+                        "1 (the reference's rho = 1, src/submodeling2.f90:93)"),
+            "parallelism": f"shots x{world} (para_range, no collective)",
+            "stage_a_history": (f"windows of {args.checkpoint} steps (checkpointed)"
+                                if args.checkpoint > 0 else "whole record"),
+            "l2": "working set (30-78 GB of FP16 history per shot) far exceeds L2"}
 
 
 def shot_dicts(pkg, h, w, ids, model_dobs=True, rho=(None, None)):
@@ -422,12 +450,8 @@ def run_ours(args):
     from daw_b200 import ranks
     rank, world, local = ranks.rank_env()
     dist = ranks.init_group(world)
-    w = make_workload(args.config, args.nt)
-    if args.maxiter is not None:
-        w.maxiter = args.maxiter
+    w = make_workload(args.config, args.nt, args.maxiter)
     reduced = args.config == 2 and (w.nt != 7500 or w.maxiter != 20)
-    if args.config == 5 and args.maxiter is None:
-        w.maxiter = 2
     # variants (reduced records, the 2001x8001 grid) skip the CPU arms
     variant = reduced or args.config == 5
     cfg1 = None
@@ -608,28 +632,17 @@ def run_ours(args):
             "scaling": "weak", "vs_baseline": None,
             "dtype": "f32 stencil / f16 history / f64 scalars",
             "data": "synthetic (seeded; observed data modelled in the true model)",
-            "config": {"workload": workload_text(w, args),
-                       "shots_per_step": [int(x) for x in step_shots],
-                       "shots_timed": int(shots_done),
-                       "batching": ("shots sorted by record length, as many per batch as HBM "
-                                    "admits, batches in seeded shuffled order"
-                                    if args.config == 4 else f"{args.batch} shots per batch"),
-                       "density": ("Gardner, rho = 0.31 vp^0.25 of each velocity model (the "
-                                   "configuration's; the reference runs rho = 1)"
-                                   if args.density == "gardner" else
-                                   "1 (the reference's rho = 1, src/submodeling2.f90:93)"),
-                       "kernel": {"auto": "TMA time-step kernels, family and launch shape "
-                                          "autotuned per mode",
-                                  "split": "TMA pressure and velocity kernels, shots per launch "
-                                           "and CTAs per SM autotuned per mode",
-                                  "step": "one TMA kernel per time step (p recomputed on the "
-                                          "v halo)"}[args.kernel]
-                                 + (", programmatic dependent launch" if args.pdl else ""),
-                       "autotuned": tc,
-                       "parallelism": f"shots x{world} (para_range, no collective)",
-                       "stage_a_history": (f"windows of {args.checkpoint} steps (checkpointed)"
-                                           if args.checkpoint > 0 else "whole record"),
-                       "l2": "working set (30-78 GB of FP16 history per shot) far exceeds L2"},
+            "config": bench_config(w, args, world),
+            "run": {"shots_per_step": [int(x) for x in step_shots],
+                    "shots_timed": int(shots_done),
+                    "kernel": {"auto": "TMA time-step kernels, family and launch shape "
+                                       "autotuned per mode",
+                               "split": "TMA pressure and velocity kernels, shots per launch "
+                                        "and CTAs per SM autotuned per mode",
+                               "step": "one TMA kernel per time step (p recomputed on the "
+                                       "v halo)"}[args.kernel]
+                              + (", programmatic dependent launch" if args.pdl else ""),
+                    "autotuned": tc},
             "clocks": clk.summary(),
             "e2e": e2e,
             "gpu_launches": int(tim["kernel_launches"]),
@@ -653,7 +666,7 @@ def run_reference(args):
     rank, world = env_int("RANK", 0), env_int("WORLD_SIZE", 1)
     if rank != 0:
         return
-    w = make_workload(args.config, args.nt)
+    w = make_workload(args.config, args.nt, args.maxiter)
     K, W = args.steps, args.warmup
     vals = []
     for i in range(W + K):
@@ -666,7 +679,7 @@ def run_reference(args):
     out = {"metric": METRIC, "value": value, "unit": "shots/hour", "n_gpus": world,
            "steps": K, "warmup": W, "higher_is_better": True, "impl": "reference",
            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-           "config": {"workload": workload_text(w, args)},
+           "config": bench_config(w, args, world),
            "cpu_baseline": {"value": value, "unit": "shots/hour", "cores": r["cores"],
                             "kind": "port", "sample": r["sample"]},
            "e2e": {"value": value, "unit": "shots/hour", "h2d_bytes_per_step": 0,

@@ -77,3 +77,19 @@ def test_gardner_density():
     assert rt.shape == (3, 4) and abs(float(rt[0, 0]) - 0.31 * 2000.0 ** 0.25) < 1e-5
     assert abs(float(r0[0, 0]) - 0.31 * 1500.0 ** 0.25) < 1e-5
     assert b.densities(w, SimpleNamespace(density="1")) == (None, None)
+
+
+def test_reference_arm_prints_the_same_config():
+    """Both arms describe the workload with one dict (bench_config), so the
+    reference arm's line carries exactly the config of the measured arm."""
+    import json
+    from types import SimpleNamespace
+    b = _bench()
+    r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference",
+                        "--steps", "1", "--warmup", "0", "--ref-sample-nt", "2", "--cpu-procs", "2"],
+                       capture_output=True, text=True, cwd=ROOT, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    line = json.loads([x for x in r.stdout.splitlines() if x.startswith("{")][-1])
+    args = SimpleNamespace(config=4, batch=2, density="1", checkpoint=0)
+    assert line["config"] == b.bench_config(b.make_workload(4), args, 1)
+    assert line["impl"] == "reference" and line["steps"] == 1
