@@ -171,3 +171,15 @@ def test_density_contrast_reflection(O, rho2):
     assert abs(R - expect) < 0.03, (R, expect)
     # arrival time within a few samples of the image wave's
     assert abs(int(np.argmax(np.abs(refl))) - int(np.argmax(np.abs(image)))) <= 8
+
+
+def test_density_fp32_vs_fp64(O):
+    """With a varying (Gardner) density the FP32 restatement stays within
+    1e-5 of the FP64 one, as with density 1."""
+    vp, npml, h, dt, nt = _case()
+    ir, is5, s = _sources(O, vp, npml, h, nt)
+    rho = np.asfortranarray((0.31 * vp.astype(np.float64) ** 0.25).astype(np.float32))
+    with O.density(rho):
+        a, _ = O.submodeling(vp, npml, h, 1, nt, dt, s, is5, ir)
+        b, _ = O.submodeling(vp, npml, h, 1, nt, dt, s, is5, ir, prec="f64")
+    assert rel_l2(a, b) <= 1e-5
